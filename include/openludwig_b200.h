@@ -1,0 +1,286 @@
+/*
+ * openludwig_b200.h -- C ABI of the B200 (sm_100a) lattice Boltzmann time step.
+ *
+ * Every entry point is plain C: raw pointers, sizes and POD structs, an int
+ * status (0 = OL_OK) and a thread-local message from ol_last_error().  No
+ * C++ types or exceptions cross this boundary and the library never frees
+ * memory it did not allocate.
+ *
+ * Drop-in layer (ol_stream_collide, ol_bouzidi, ol_thermal, ol_surface_forces,
+ * ol_init_equilibrium, ol_flow_stats): all pointers are DEVICE pointers to
+ * buffers laid out exactly like the reference's Julia column-major CuArrays,
+ * so `pointer(::CuArray)` can be handed over unchanged:
+ *     f[x,y,z,b,k]  -> (x-1) + 8(y-1) + 64(z-1) + 512(b-1) + 512*nB*(k-1)
+ *     vel[x,y,z,b,c]-> same with c in 1..3;  rho/obstacle/sponge/wall_dist[x,y,z,b]
+ *     neighbor_table[b,dir] -> (b-1) + nB*(dir-1), dir=(dx+1)+3(dy+1)+9(dz+1)+1
+ *     block_pointer[bx,by,bz] -> dense Int32 grid, bx fastest
+ * Index VALUES stored inside those arrays keep the reference's 1-based
+ * convention (block ids 1..nB, 0 = missing; Bouzidi cell x/y/z in 1..8).
+ * The block edge is fixed at 8 cells (blocks.jl BLOCK_SIZE).
+ *
+ * Native layer (ol_ctx_*, ol_batch_*): the library owns a device block pool
+ * with FP32 or FP16-shifted population storage, advances many cases of uneven
+ * size together with persistent kernels replayed from a CUDA graph, and is
+ * driven by the Python request loop in openludwig_b200.serving.
+ */
+#ifndef OPENLUDWIG_B200_H
+#define OPENLUDWIG_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define OL_API __attribute__((visibility("default")))
+#else
+#define OL_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define OL_OK 0
+#define OL_ERR_ARG 1        /* bad argument (null pointer, size, enum)        */
+#define OL_ERR_CUDA 2       /* a CUDA runtime call failed                      */
+#define OL_ERR_NOMEM 3      /* allocation or HBM budget exceeded               */
+#define OL_ERR_STATE 4      /* call out of order / unknown handle              */
+#define OL_ERR_NUMERIC 5    /* device watchdog: NaN or rho below threshold     */
+
+/* collision operators (physics_kernels.jl:35-45) */
+#define OL_OP_CUMULANT 0
+#define OL_OP_REGULARIZED_BGK 1
+/* cumulant limiter (timestep.jl:46-47) */
+#define OL_LIMITER_NONE 0
+#define OL_LIMITER_FACTORED 1
+#define OL_LIMITER_POSITIVITY 2
+
+/* ------------------------------------------------------------------ */
+/* Drop-in layer                                                        */
+/* ------------------------------------------------------------------ */
+
+/* One refinement level's device buffers (the BlockLevel fields the flow
+ * kernel reads and writes, blocks.jl:138-196). */
+typedef struct ol_level_view {
+  float *f_out;                 /* [512*nB*27] written                        */
+  const float *f_in;            /* [512*nB*27] read (pull source)             */
+  float *f_post;                /* [512*nB*27] post-collision copy, or NULL    */
+  float *rho;                   /* [512*nB]    written                         */
+  float *vel_out;               /* [512*nB*3]  written                         */
+  const float *vel_in;          /* [512*nB*3]  read (WALE gradients)           */
+  const uint8_t *obstacle;      /* [512*nB]    Julia Bool                      */
+  const float *sponge;          /* [512*nB]                                    */
+  const float *wall_dist;       /* [512*nB]    may be NULL if no wall model    */
+  const int32_t *neighbor_table;/* [nB*27]     1-based ids, 0 = missing        */
+  const int32_t *map_x, *map_y, *map_z; /* [nB] 1-based block coordinates     */
+  int32_t n_blocks;
+} ol_level_view;
+
+/* Parent-level state for coarse-to-fine ghost interpolation
+ * (physics_interpolation.jl:4-127).  Ignored when is_level_1 != 0. */
+typedef struct ol_parent_view {
+  const float *f, *rho, *vel;           /* parent state after its step        */
+  const float *f_old, *rho_old, *vel_old; /* parent state before its step     */
+  const int32_t *block_ptr;             /* [dim_x*dim_y*dim_z] 1-based ids    */
+  int32_t dim_x, dim_y, dim_z;          /* size(block_ptr)                    */
+  int32_t n_blocks;                     /* parent nB (array stride)           */
+} ol_parent_view;
+
+/* Every scalar argument of stream_collide_cumulant! (kernel_cumulant.jl:38-68);
+ * the regularized-BGK kernel takes the same list (kernel_regularized_bgk.jl:13-41). */
+typedef struct ol_step_params {
+  int32_t op;                   /* OL_OP_*                                    */
+  float tau_molecular, tau_parent, c_wale, nu_sgs_background;
+  int32_t is_level_1, is_symmetric;
+  int32_t nx_global, ny_global, nz_global;
+  float u_inlet;
+  int32_t wall_model_active, time_step_seed, store_post_collision;
+  float inlet_turbulence, temporal_weight;
+  int32_t use_temporal_interp, sponge_blend_distributions;
+  float omega_bulk, omega_3, omega_4;
+  int32_t adaptive_omega4;
+  float lambda_param;
+  int32_t limiter_type, compressible_corr;
+} ol_step_params;
+
+/* Fused pull-stream + collision of one level sub-step: one launch, grid of
+ * one CTA per 8^3 block.  Replaces the kernel launch in perform_timestep_v2!
+ * (timestep.jl:51-88, kernel_cumulant.jl:29-627 / kernel_regularized_bgk.jl:4-325).
+ * `stream` is a cudaStream_t (NULL = legacy default stream). */
+OL_API int ol_stream_collide(const ol_level_view *lv, const ol_parent_view *pv,
+                      const ol_step_params *sp, void *stream);
+
+/* Bouzidi interpolated bounce-back (bouzidi_kernel.jl:13-122).  q_map holds
+ * IEEE binary16 bit patterns [512*nB*27]; cell_* are the sparse boundary-cell
+ * lists (block 1-based Int32, x/y/z 1-based Int8).  Reads f_post, writes f_out. */
+OL_API int ol_bouzidi(float *f_out, const float *f_post, const uint16_t *q_map,
+               const int32_t *cell_block, const int8_t *cell_x,
+               const int8_t *cell_y, const int8_t *cell_z, int32_t n_boundary,
+               const int32_t *neighbor_table, int32_t n_blocks,
+               float q_min_threshold, void *stream);
+
+/* Same result as ol_bouzidi without a dense post-collision copy: f_out still
+ * holds the post-collision values when it is called (the flow kernel ran with
+ * store_post_collision = 0).  Phase 1 gathers every corrected link into
+ * `scratch` (>= 27*n_boundary floats, caller-owned device memory), phase 2
+ * scatters them, so no link reads a value another link already replaced.
+ * Replaces the f_post_collision round trip of timestep.jl:71 + :90-98. */
+OL_API int ol_bouzidi_sparse(float *f_out, const uint16_t *q_map,
+                      const int32_t *cell_block, const int8_t *cell_x,
+                      const int8_t *cell_y, const int8_t *cell_z,
+                      int32_t n_boundary, const int32_t *neighbor_table,
+                      int32_t n_blocks, float q_min_threshold, float *scratch,
+                      void *stream);
+
+/* Thermal DDF level view + parameters (kernel_thermal.jl:14-40). */
+typedef struct ol_thermal_view {
+  float *g_out; const float *g_in; float *g_post;  /* g_post may be NULL     */
+  float *temperature;            /* [512*nB] written                          */
+  const float *vel;              /* flow kernel's vel_out of this sub-step    */
+  const uint8_t *obstacle; const float *sponge;
+  const int32_t *neighbor_table; const int32_t *map_x, *map_y, *map_z;
+  int32_t n_blocks;
+  /* parent (coarse-to-fine, physics_interpolation.jl:135-247) */
+  const float *pg, *pT, *pvel, *pg_old, *pT_old, *pvel_old;
+  const int32_t *p_block_ptr; int32_t p_dim_x, p_dim_y, p_dim_z, p_n_blocks;
+} ol_thermal_view;
+
+typedef struct ol_thermal_params {
+  float tau_g, tau_g_parent;
+  int32_t is_level_1, is_symmetric, nx_global, ny_global, nz_global;
+  float u_inlet, T_inlet, T_wall;
+  int32_t wall_bc_adiabatic, store_post_collision;
+  float temporal_weight;
+  int32_t use_temporal_interp, sponge_blend_distributions;
+} ol_thermal_params;
+
+/* Thermal DDF stream-collide (kernel_thermal.jl:14-202). */
+OL_API int ol_thermal(const ol_thermal_view *tv, const ol_thermal_params *tp,
+               void *stream);
+
+/* Initial state of a level (main.jl:113-150): f = f_temp = w_k, and when
+ * f_old != NULL also f_old = w_k, rho_old = 1, vel_old = 0. */
+OL_API int ol_init_equilibrium(float *f, float *f_temp, float *f_old, float *rho_old,
+                        float *vel_old, int32_t n_blocks, void *stream);
+
+/* Surface mesh on the device (geometry.jl:24-33 GPUMesh). */
+typedef struct ol_surface_mesh {
+  const float *cx, *cy, *cz;     /* triangle centres (unrotated domain frame) */
+  const float *nx, *ny, *nz;     /* unit normals                              */
+  const float *area;
+  int32_t n_triangles;
+} ol_surface_mesh;
+
+typedef struct ol_force_params {
+  float dx;                              /* Float32(level.dx)                  */
+  int32_t dim_x, dim_y, dim_z;           /* level grid_dim (size(block_ptr))   */
+  float offset_x, offset_y, offset_z;    /* mesh_offset                        */
+  float pressure_scale, stress_scale;    /* rho_phys * U_vs^2                  */
+  float tau_molecular;
+  int32_t search_radius;
+  float c_wale, nu_sgs_bg;
+  float ref_x, ref_y, ref_z;             /* moment centre                      */
+} ol_force_params;
+
+/* map_stresses_kernel! + integrate_forces_kernel! (surface.jl:350-507,
+ * 702-762).  Writes the per-triangle maps (p, tau_x, tau_y, tau_z, device
+ * arrays of n_triangles) and out[9] = {Fx_p, Fy_p, Fz_p, Fx_v, Fy_v, Fz_v,
+ * Mx, My, Mz} summed in FP64 in a fixed order (deterministic; the
+ * reference's FP32 atomics are not).  `partials` is caller device scratch of
+ * >= ol_surface_forces_scratch_doubles(n_triangles) doubles. */
+OL_API int ol_surface_forces(const ol_surface_mesh *mesh, const float *rho,
+                      const float *vel, const uint8_t *obstacle,
+                      const int32_t *block_ptr, int32_t n_blocks,
+                      const ol_force_params *fp, float *p_map, float *sx_map,
+                      float *sy_map, float *sz_map, double *partials,
+                      double out[9], void *stream);
+OL_API size_t ol_surface_forces_scratch_doubles(int32_t n_triangles);
+
+/* Flow statistics of a level in FP64 (diagnostics.jl:43-93):
+ * out[0..6] = {n_fluid, rho_sum, rho_min, rho_max, v_max, kinetic_energy,
+ * mass_all_cells}.  `partials` >= ol_flow_stats_scratch_doubles(nB). */
+OL_API int ol_flow_stats(const float *rho, const float *vel, const uint8_t *obstacle,
+                  int32_t n_blocks, double *partials, double out[7],
+                  void *stream);
+OL_API size_t ol_flow_stats_scratch_doubles(int32_t n_blocks);
+
+/* ------------------------------------------------------------------ */
+/* Native layer: device block pool, FP16-shifted storage, batched       */
+/* multi-case stepping with persistent kernels and CUDA graphs.         */
+/* ------------------------------------------------------------------ */
+
+#define OL_STORE_F32 0
+#define OL_STORE_F16 1   /* f stored as binary16 of (f_k/w_k - 1) * scale */
+
+typedef struct ol_ctx ol_ctx;
+
+/* Host description of one refinement level of one case.  Arrays are HOST
+ * memory in the drop-in layout above; the library copies them. */
+typedef struct ol_level_desc {
+  int32_t n_blocks;
+  const int32_t *map_x, *map_y, *map_z;     /* [nB] 1-based                   */
+  const int32_t *neighbor_table;            /* [nB*27]                         */
+  const int32_t *block_ptr;                 /* [dim_x*dim_y*dim_z]             */
+  int32_t dim_x, dim_y, dim_z;
+  const uint8_t *obstacle;                  /* [512*nB]                        */
+  const float *sponge;                      /* [512*nB]                        */
+  const float *wall_dist;                   /* [512*nB] or NULL                */
+  /* Bouzidi (dense q-map of binary16 bits + sparse cell list) or n_boundary=0 */
+  int32_t n_boundary;
+  const uint16_t *q_map;                    /* [512*nB*27]                     */
+  const int32_t *cell_block; const int8_t *cell_x, *cell_y, *cell_z;
+  float tau;                                /* tau of this level               */
+  float tau_g;                              /* thermal tau (DDF cases)         */
+  float store_scale;                        /* FP16 shift scale of this level  */
+} ol_level_desc;
+
+typedef struct ol_case_desc {
+  int32_t n_levels;
+  const ol_level_desc *levels;              /* [n_levels], coarsest first      */
+  int32_t nx, ny, nz;                       /* coarse domain size in cells     */
+  ol_step_params params;                    /* shared scalars (tau fields unused) */
+  int32_t ddf;                              /* thermal DDF on                  */
+  ol_thermal_params tparams;                /* thermal scalars (taus unused)   */
+  /* surface mesh (host arrays, n_triangles entries) for Cd/Cl */
+  int32_t n_triangles;
+  const float *tri_cx, *tri_cy, *tri_cz, *tri_nx, *tri_ny, *tri_nz, *tri_area;
+  ol_force_params force;                    /* finest-level force parameters   */
+  float u_target;                           /* lattice inlet speed after ramp  */
+  int32_t ramp_steps;                       /* cosine ramp (main.jl:217)       */
+  int32_t async_depth;                      /* ramp batching (main.jl:210-218) */
+} ol_case_desc;
+
+OL_API int ol_ctx_create(ol_ctx **out, int device, size_t hbm_budget_bytes,
+                  int store_kind);
+OL_API int ol_ctx_destroy(ol_ctx *ctx);
+/* bytes of device memory a case would take in this context */
+OL_API int ol_ctx_case_footprint(ol_ctx *ctx, const ol_case_desc *cd, size_t *bytes);
+OL_API int ol_ctx_case_add(ol_ctx *ctx, const ol_case_desc *cd, int32_t *case_id);
+OL_API int ol_ctx_case_remove(ol_ctx *ctx, int32_t case_id);
+/* Advance every resident case by n_coarse coarse steps (one graph replay
+ * per coarse step).  Asynchronous on the context stream. */
+OL_API int ol_ctx_step(ol_ctx *ctx, int32_t n_coarse);
+OL_API int ol_ctx_sync(ol_ctx *ctx);
+/* Surface forces of one case on its finest level: out[9] as ol_surface_forces. */
+OL_API int ol_ctx_case_forces(ol_ctx *ctx, int32_t case_id, double out[9]);
+/* Download a level's macroscopic fields (host buffers of 512*nB / 512*nB*3),
+ * populations (host [512*nB*27] FP32, decoded), or NULL to skip. */
+OL_API int ol_ctx_case_download(ol_ctx *ctx, int32_t case_id, int32_t level,
+                         float *rho, float *vel, float *f);
+/* Coarse steps a case has done, and its device watchdog status. */
+OL_API int ol_ctx_case_info(ol_ctx *ctx, int32_t case_id, int64_t *coarse_steps,
+                     int32_t *status);
+/* Launch-shape autotuning over persistent grid sizes; result is kept. */
+OL_API int ol_ctx_autotune(ol_ctx *ctx, int32_t trials);
+/* Bytes in use / budget / number of resident cases / kernel launches issued. */
+OL_API int ol_ctx_stats(ol_ctx *ctx, size_t *used, size_t *budget, int32_t *n_cases,
+                 int64_t *launches);
+
+/* Message of the last failing call on this thread. */
+OL_API const char *ol_last_error(void);
+/* Library version string. */
+OL_API const char *ol_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* OPENLUDWIG_B200_H */

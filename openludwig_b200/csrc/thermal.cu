@@ -1,0 +1,84 @@
+// Thermal DDF launch and its C ABI (stream_collide_thermal!, timestep.jl:101-145).
+#include "common.cuh"
+#include "thermal.cuh"
+
+namespace ol {
+
+constexpr int kGhostBytesT = 27 * BCELLS * sizeof(float);
+
+template <class ST>
+__global__ void __launch_bounds__(512, 2) k_thermal(const __grid_constant__ ThermalDev D) {
+  __shared__ int nb_blk[27];
+  __shared__ int n_missing;
+  extern __shared__ float ghost[];
+  const int b = blockIdx.x;
+  if (threadIdx.x == 0) n_missing = 0;
+  __syncthreads();
+  if (threadIdx.x < 27) {
+    const int nb = D.nbr[b + D.nbr_stride * threadIdx.x];
+    nb_blk[threadIdx.x] = nb;
+    if (nb <= 0) atomicAdd(&n_missing, 1);
+  }
+  __syncthreads();
+  if (n_missing) fill_ghost_thermal<ST>(D, nb_blk, b, threadIdx.x, ghost);
+  thermal_cell<ST>(D, nb_blk, ghost, b, threadIdx.x);
+}
+
+template <class ST>
+static void launch_t(const ThermalDev &D, cudaStream_t s) {
+  static bool done = false;
+  if (!done) {
+    cudaFuncSetAttribute(k_thermal<ST>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         kGhostBytesT);
+    done = true;
+  }
+  k_thermal<ST><<<D.n_blocks, BCELLS, kGhostBytesT, s>>>(D);
+}
+
+void launch_thermal(const ThermalDev &D, bool f16, cudaStream_t s) {
+  if (D.n_blocks <= 0) return;
+  if (f16) launch_t<StoreF16S>(D, s);
+  else launch_t<StoreF32>(D, s);
+}
+
+}  // namespace ol
+
+using namespace ol;
+
+extern "C" int ol_thermal(const ol_thermal_view *tv, const ol_thermal_params *tp, void *stream) {
+  OL_CHECK_ARG(tv && tp, "ol_thermal: null view or params");
+  OL_CHECK_ARG(tv->n_blocks >= 0, "ol_thermal: n_blocks < 0");
+  if (tv->n_blocks == 0) return OL_OK;
+  OL_CHECK_ARG(tv->g_in && tv->g_out && tv->temperature && tv->vel && tv->obstacle &&
+                   tv->sponge && tv->neighbor_table && tv->map_x && tv->map_y && tv->map_z,
+               "ol_thermal: required buffer is null");
+  OL_CHECK_ARG(tv->g_in != tv->g_out, "ol_thermal: g_in aliases g_out");
+  OL_CHECK_ARG(!(tp->store_post_collision == 1) || tv->g_post,
+               "ol_thermal: store_post_collision needs g_post");
+  ThermalDev D = {};
+  D.g_in = tv->g_in; D.g_out = tv->g_out; D.g_post = tv->g_post;
+  D.T_out = tv->temperature; D.vel = tv->vel; D.obstacle = tv->obstacle; D.sponge = tv->sponge;
+  D.nbr = tv->neighbor_table; D.map_x = tv->map_x; D.map_y = tv->map_y; D.map_z = tv->map_z;
+  D.n_blocks = tv->n_blocks;
+  D.block_offset = 0;
+  D.dstride = (int64_t)BCELLS * tv->n_blocks;
+  D.nbr_stride = tv->n_blocks;
+  D.scale = 1.0f; D.inv_scale = 1.0f; D.p_inv_scale = 1.0f;
+  D.tp = *tp;
+  if (!tp->is_level_1) {
+    OL_CHECK_ARG(tv->pg && tv->pT && tv->pvel && tv->p_block_ptr && tv->p_n_blocks > 0,
+                 "ol_thermal: fine level needs parent thermal state");
+    OL_CHECK_ARG(!(tp->use_temporal_interp == 1 && tp->temporal_weight < 0.99f) ||
+                     (tv->pg_old && tv->pT_old && tv->pvel_old),
+                 "ol_thermal: temporal interpolation needs parent old state");
+    D.pg = tv->pg; D.pT = tv->pT; D.pvel = tv->pvel;
+    D.pg_old = tv->pg_old; D.pT_old = tv->pT_old; D.pvel_old = tv->pvel_old;
+    D.pptr = tv->p_block_ptr;
+    D.pdim_x = tv->p_dim_x; D.pdim_y = tv->p_dim_y; D.pdim_z = tv->p_dim_z;
+    D.p_block_offset = 0;
+    D.p_dstride = (int64_t)BCELLS * tv->p_n_blocks;
+  }
+  launch_thermal(D, false, (cudaStream_t)stream);
+  OL_LAUNCHED("ol_thermal");
+  return OL_OK;
+}

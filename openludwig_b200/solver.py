@@ -1,0 +1,339 @@
+"""Device-resident levels and the time-step driver, mirroring the reference's
+solver path through the C ABI:
+
+  perform_timestep_v2!   (collision/timestep.jl:1-159)  -> perform_timestep
+  recursive_step!        (solver/solver_control.jl:6-98) -> recursive_step
+  execute_timestep_batch! (solver_control.jl:199-218)   -> execute_timestep_batch
+  main.jl:208-315 loop (ramp, diagnostics, forces)      -> Simulation.run
+
+Buffers are torch CUDA tensors in the reference layout; every kernel is a
+call into libopenludwig_b200.so on the current torch stream.  There is no
+CPU fallback: without a CUDA device or the built library the calls raise.
+
+Differences from the reference that do not change results:
+  * copy_to_old! (blocks.jl:241-252) copies f_in and vel_in before a parent
+    step; the children only read that state while the parent's f_in is
+    untouched, so f_old / vel_old alias f_in / vel_in and only rho (which the
+    step overwrites in place) is copied.
+  * Bouzidi runs in the sparse two-phase form (gather corrected links, then
+    scatter) so the dense post-collision copy f_post is never written.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import dataclasses as dc
+import math
+
+import numpy as np
+import torch
+
+from . import _native as N
+from .config import CaseConfig
+from .domain import HostLevel
+from .scaling import DomainParams
+
+BS = 8
+
+
+def _ptr(t: torch.Tensor | None):
+    return None if t is None else C.c_void_p(t.data_ptr())
+
+
+def _stream():
+    return C.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+@dc.dataclass
+class DeviceLevel:
+    host: HostLevel
+    f: torch.Tensor
+    f_temp: torch.Tensor
+    rho: torch.Tensor
+    rho_old: torch.Tensor
+    vel: torch.Tensor
+    vel_temp: torch.Tensor
+    obstacle: torch.Tensor
+    sponge: torch.Tensor
+    wall_dist: torch.Tensor
+    neighbor_table: torch.Tensor
+    map_x: torch.Tensor
+    map_y: torch.Tensor
+    map_z: torch.Tensor
+    block_ptr: torch.Tensor
+    q_map: torch.Tensor | None = None
+    cell_block: torch.Tensor | None = None
+    cell_x: torch.Tensor | None = None
+    cell_y: torch.Tensor | None = None
+    cell_z: torch.Tensor | None = None
+    bouzidi_scratch: torch.Tensor | None = None
+    f_post: torch.Tensor | None = None
+    # thermal DDF
+    g: torch.Tensor | None = None
+    g_temp: torch.Tensor | None = None
+    temperature: torch.Tensor | None = None
+    temperature_old: torch.Tensor | None = None
+    # aliases of the parent state read by the children (set per step)
+    f_old: torch.Tensor | None = None
+    vel_old: torch.Tensor | None = None
+    g_old: torch.Tensor | None = None
+
+    @property
+    def n_blocks(self) -> int:
+        return self.host.n_blocks
+
+    @property
+    def tau(self) -> float:
+        return self.host.tau
+
+    @property
+    def has_bouzidi(self) -> bool:
+        return self.host.bouzidi and self.host.n_boundary > 0
+
+
+def upload_level(h: HostLevel, device: torch.device, ddf: bool = False, t_init: float = 1.0,
+                 reference_bouzidi: bool = False) -> DeviceLevel:
+    """adapt(backend, g) + the initial state of main.jl:113-173."""
+    n = h.n_blocks
+    S = 512 * n
+    dev = device
+    t = lambda a, dt=None: torch.from_numpy(np.ascontiguousarray(a)).to(dev)  # noqa: E731
+    f = torch.empty(S * 27, dtype=torch.float32, device=dev)
+    ft = torch.empty_like(f)
+    rho_old = torch.ones(S, dtype=torch.float32, device=dev)
+    vel_old = torch.zeros(S * 3, dtype=torch.float32, device=dev)
+    f_old = torch.empty_like(f)
+    N.call("ol_init_equilibrium", _ptr(f), _ptr(ft), _ptr(f_old), _ptr(rho_old), _ptr(vel_old),
+           N.i32(n), _stream())
+    del f_old, vel_old
+    lv = DeviceLevel(
+        host=h, f=f, f_temp=ft,
+        rho=torch.ones(S, dtype=torch.float32, device=dev), rho_old=rho_old,
+        vel=torch.zeros(S * 3, dtype=torch.float32, device=dev),
+        vel_temp=torch.zeros(S * 3, dtype=torch.float32, device=dev),
+        obstacle=t(h.obstacle), sponge=t(h.sponge), wall_dist=t(h.wall_dist),
+        neighbor_table=t(h.neighbor_table), map_x=t(h.map_x), map_y=t(h.map_y),
+        map_z=t(h.map_z), block_ptr=t(h.block_ptr))
+    if h.bouzidi and h.n_boundary > 0:
+        lv.q_map = t(h.q_map.view(np.int16))
+        lv.cell_block, lv.cell_x = t(h.cell_block), t(h.cell_x)
+        lv.cell_y, lv.cell_z = t(h.cell_y), t(h.cell_z)
+        lv.bouzidi_scratch = torch.empty(27 * h.n_boundary, dtype=torch.float32, device=dev)
+        if reference_bouzidi:
+            lv.f_post = torch.zeros(S * 27, dtype=torch.float32, device=dev)
+    if ddf:
+        w = torch.tensor(lattice_weights(), dtype=torch.float32, device=dev)
+        lv.g = (w[:, None] * t_init).expand(27, S).reshape(-1).clone()
+        lv.g_temp = lv.g.clone()
+        lv.temperature = torch.full((S,), t_init, dtype=torch.float32, device=dev)
+        lv.temperature_old = lv.temperature.clone()
+    return lv
+
+
+def lattice_weights() -> list:
+    out = []
+    for cz in (-1, 0, 1):
+        for cy in (-1, 0, 1):
+            for cx in (-1, 0, 1):
+                d2 = cx * cx + cy * cy + cz * cz
+                num, den = ((8, 27) if d2 == 0 else (2, 27) if d2 == 1 else (1, 54) if d2 == 2
+                            else (1, 216))
+                out.append(float(np.float32(num) / np.float32(den)))
+    return out
+
+
+@dc.dataclass
+class StepSettings:
+    """The scalars perform_timestep_v2! reads from globals (timestep.jl:39-49)."""
+    op: int = 0
+    c_wale: float = 0.2
+    nu_sgs_bg: float = 0.0
+    is_symmetric: int = 0
+    wall_model: int = 0
+    inlet_turbulence: float = 0.0
+    use_temporal_interp: int = 1
+    sponge_blend: int = 0
+    omega_bulk: float = 1.0
+    omega_3: float = 1.0
+    omega_4: float = 1.0
+    adaptive_omega4: int = 1
+    lambda_param: float = 1.0 / 6.0
+    limiter: int = 1
+    compressible: int = 0
+    q_min: float = 0.001
+    ddf: int = 0
+    t_inlet: float = 1.0
+    t_wall: float = 1.0
+    wall_bc_adiabatic: int = 1
+
+    @staticmethod
+    def from_config(cfg: CaseConfig, wall_model_active: bool) -> "StepSettings":
+        return StepSettings(op=cfg.operator_code, c_wale=cfg.c_wale, nu_sgs_bg=cfg.nu_sgs_background,
+                            is_symmetric=int(cfg.symmetric_analysis), wall_model=int(wall_model_active),
+                            inlet_turbulence=cfg.inlet_turbulence_intensity,
+                            use_temporal_interp=int(cfg.temporal_interpolation),
+                            sponge_blend=int(cfg.sponge_blend_distributions),
+                            omega_bulk=cfg.cumulant_omega_bulk, omega_3=cfg.cumulant_omega_3,
+                            omega_4=cfg.cumulant_omega_4,
+                            adaptive_omega4=int(cfg.cumulant_adaptive_omega4),
+                            lambda_param=cfg.cumulant_lambda_param, limiter=cfg.limiter_code,
+                            compressible=int(cfg.compressibility_correction),
+                            q_min=cfg.q_min_threshold, ddf=int(cfg.ddf_enabled),
+                            t_inlet=cfg.ddf_t_inlet, t_wall=cfg.ddf_t_wall,
+                            wall_bc_adiabatic=int(cfg.ddf_wall_bc == "adiabatic"))
+
+
+def step_params(s: StepSettings, lv: DeviceLevel, parent_tau: float, is_l1: bool, dims, u: float,
+                t_sub: int, tw: float, store_post: bool) -> N.StepParams:
+    sp = N.StepParams()
+    sp.op = s.op
+    sp.tau_molecular = lv.tau
+    sp.tau_parent = parent_tau
+    sp.c_wale = s.c_wale
+    sp.nu_sgs_background = s.nu_sgs_bg
+    sp.is_level_1 = int(is_l1)
+    sp.is_symmetric = s.is_symmetric
+    sp.nx_global, sp.ny_global, sp.nz_global = dims
+    sp.u_inlet = u
+    sp.wall_model_active = s.wall_model
+    sp.time_step_seed = t_sub % 1000000
+    sp.store_post_collision = int(store_post)
+    sp.inlet_turbulence = s.inlet_turbulence
+    sp.temporal_weight = tw
+    sp.use_temporal_interp = s.use_temporal_interp
+    sp.sponge_blend_distributions = s.sponge_blend
+    sp.omega_bulk, sp.omega_3, sp.omega_4 = s.omega_bulk, s.omega_3, s.omega_4
+    sp.adaptive_omega4 = s.adaptive_omega4
+    sp.lambda_param = s.lambda_param
+    sp.limiter_type = s.limiter
+    sp.compressible_corr = s.compressible
+    return sp
+
+
+@dc.dataclass
+class ParentRef:
+    lv: DeviceLevel
+    f_new: torch.Tensor
+    vel_new: torch.Tensor
+    g_new: torch.Tensor | None
+
+
+def perform_timestep(s: StepSettings, lv: DeviceLevel, parent: ParentRef | None, f_out, f_in,
+                     vel_out, vel_in, u: float, t_sub: int, tw: float, domain_dims,
+                     g_out=None, g_in=None) -> None:
+    """timestep.jl:1-159: flow kernel, Bouzidi, thermal kernel, thermal Bouzidi."""
+    n = lv.n_blocks
+    if n == 0:
+        return
+    is_l1 = parent is None
+    scale = 1 << (lv.host.level_id - 1)
+    dims = (domain_dims[0] * scale, domain_dims[1] * scale, domain_dims[2] * scale)
+    ref_post = lv.f_post is not None
+    sp = step_params(s, lv, parent.lv.tau if parent else 0.5, is_l1, dims, u, t_sub, tw,
+                     lv.has_bouzidi and ref_post)
+    view = N.LevelView(f_out=_ptr(f_out), f_in=_ptr(f_in), f_post=_ptr(lv.f_post),
+                       rho=_ptr(lv.rho), vel_out=_ptr(vel_out), vel_in=_ptr(vel_in),
+                       obstacle=_ptr(lv.obstacle), sponge=_ptr(lv.sponge),
+                       wall_dist=_ptr(lv.wall_dist), neighbor_table=_ptr(lv.neighbor_table),
+                       map_x=_ptr(lv.map_x), map_y=_ptr(lv.map_y), map_z=_ptr(lv.map_z),
+                       n_blocks=n)
+    pv = N.ParentView()
+    if parent is not None:
+        p = parent.lv
+        d = p.host.grid_dim
+        pv = N.ParentView(f=_ptr(parent.f_new), rho=_ptr(p.rho), vel=_ptr(parent.vel_new),
+                          f_old=_ptr(p.f_old), rho_old=_ptr(p.rho_old), vel_old=_ptr(p.vel_old),
+                          block_ptr=_ptr(p.block_ptr), dim_x=d[0], dim_y=d[1], dim_z=d[2],
+                          n_blocks=p.n_blocks)
+    st = _stream()
+    N.call("ol_stream_collide", C.byref(view), C.byref(pv), C.byref(sp), st)
+    if lv.has_bouzidi:
+        h = lv.host
+        if ref_post:
+            N.call("ol_bouzidi", _ptr(f_out), _ptr(lv.f_post), _ptr(lv.q_map), _ptr(lv.cell_block),
+                   _ptr(lv.cell_x), _ptr(lv.cell_y), _ptr(lv.cell_z), N.i32(h.n_boundary),
+                   _ptr(lv.neighbor_table), N.i32(n), N.f32(s.q_min), st)
+        else:
+            N.call("ol_bouzidi_sparse", _ptr(f_out), _ptr(lv.q_map), _ptr(lv.cell_block),
+                   _ptr(lv.cell_x), _ptr(lv.cell_y), _ptr(lv.cell_z), N.i32(h.n_boundary),
+                   _ptr(lv.neighbor_table), N.i32(n), N.f32(s.q_min), _ptr(lv.bouzidi_scratch), st)
+    if s.ddf and g_out is not None:
+        tp = N.ThermalParams(tau_g=lv.host.tau_g, tau_g_parent=parent.lv.host.tau_g if parent else 0.5,
+                             is_level_1=int(is_l1), is_symmetric=s.is_symmetric,
+                             nx_global=dims[0], ny_global=dims[1], nz_global=dims[2], u_inlet=u,
+                             T_inlet=s.t_inlet, T_wall=s.t_wall,
+                             wall_bc_adiabatic=s.wall_bc_adiabatic, store_post_collision=0,
+                             temporal_weight=tw, use_temporal_interp=s.use_temporal_interp,
+                             sponge_blend_distributions=s.sponge_blend)
+        tv = N.ThermalView(g_out=_ptr(g_out), g_in=_ptr(g_in), g_post=None,
+                           temperature=_ptr(lv.temperature), vel=_ptr(vel_out),
+                           obstacle=_ptr(lv.obstacle), sponge=_ptr(lv.sponge),
+                           neighbor_table=_ptr(lv.neighbor_table), map_x=_ptr(lv.map_x),
+                           map_y=_ptr(lv.map_y), map_z=_ptr(lv.map_z), n_blocks=n)
+        if parent is not None:
+            p = parent.lv
+            d = p.host.grid_dim
+            tv.pg, tv.pT, tv.pvel = _ptr(parent.g_new), _ptr(p.temperature), _ptr(parent.vel_new)
+            tv.pg_old, tv.pT_old, tv.pvel_old = _ptr(p.g_old), _ptr(p.temperature_old), _ptr(p.vel_old)
+            tv.p_block_ptr = _ptr(p.block_ptr)
+            tv.p_dim_x, tv.p_dim_y, tv.p_dim_z = d
+            tv.p_n_blocks = p.n_blocks
+        N.call("ol_thermal", C.byref(tv), C.byref(tp), st)
+        if lv.has_bouzidi:
+            h = lv.host
+            N.call("ol_bouzidi_sparse", _ptr(g_out), _ptr(lv.q_map), _ptr(lv.cell_block),
+                   _ptr(lv.cell_x), _ptr(lv.cell_y), _ptr(lv.cell_z), N.i32(h.n_boundary),
+                   _ptr(lv.neighbor_table), N.i32(n), N.f32(s.q_min), _ptr(lv.bouzidi_scratch), st)
+
+
+def recursive_step(levels: list, s: StepSettings, lvl: int, t_sub: int, parent: ParentRef | None,
+                   tw: float, u: float, domain_dims) -> None:
+    """solver_control.jl:6-197 (recursive_step! and recursive_step_temporal!)."""
+    if lvl >= len(levels):
+        return
+    lv = levels[lvl]
+    if t_sub % 2 == 0:
+        f_in, f_out, vel_in, vel_out = lv.f, lv.f_temp, lv.vel, lv.vel_temp
+        g_in, g_out = lv.g, lv.g_temp
+    else:
+        f_in, f_out, vel_in, vel_out = lv.f_temp, lv.f, lv.vel_temp, lv.vel
+        g_in, g_out = lv.g_temp, lv.g
+    has_children = lvl + 1 < len(levels)
+    if has_children and s.use_temporal_interp:
+        # copy_to_old!: f_old / vel_old alias the untouched pull sources
+        lv.f_old, lv.vel_old = f_in, vel_in
+        lv.rho_old.copy_(lv.rho)
+        if s.ddf and lv.g is not None:
+            lv.g_old = g_in
+            lv.temperature_old.copy_(lv.temperature)
+    perform_timestep(s, lv, parent, f_out, f_in, vel_out, vel_in, u, t_sub,
+                     0.0 if parent is None else tw, domain_dims,
+                     g_out=g_out if s.ddf else None, g_in=g_in if s.ddf else None)
+    if has_children:
+        me = ParentRef(lv, f_out, vel_out, g_out if s.ddf else None)
+        recursive_step(levels, s, lvl + 1, 2 * t_sub, me, 0.0, u, domain_dims)
+        recursive_step(levels, s, lvl + 1, 2 * t_sub + 1, me, 0.5, u, domain_dims)
+
+
+def execute_timestep_batch(levels, s: StepSettings, t_start: int, batch: int, u: float,
+                           domain_dims) -> None:
+    """solver_control.jl:199-218."""
+    for off in range(batch):
+        recursive_step(levels, s, 0, t_start + off, None, 0.0, u, domain_dims)
+
+
+def ramp_velocity(u_target: float, batch_end: int, ramp_steps: int) -> float:
+    """main.jl:217-218: cosine ramp evaluated once per batch at its end step."""
+    if ramp_steps > 0 and batch_end <= ramp_steps:
+        prog = np.float32(0.5) * (np.float32(1.0) - np.float32(math.cos(np.float32(math.pi) * batch_end / ramp_steps)))
+    else:
+        prog = np.float32(1.0)
+    return float(np.float32(u_target) * np.float32(prog))
+
+
+def cells_total(levels) -> int:
+    return sum(lv.n_blocks * 512 for lv in levels)
+
+
+def cell_updates_per_coarse_step(levels) -> int:
+    """True cell updates: level l advances 2^(l-1) times per coarse step."""
+    return sum(lv.n_blocks * 512 * (1 << i) for i, lv in enumerate(levels))

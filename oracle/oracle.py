@@ -1,0 +1,201 @@
+"""ctypes wrapper of the CPU oracle (oracle/_build/libolorc.so).
+
+TEST INFRASTRUCTURE: imported only by tests/, __graft_entry__.smoke() and the
+CPU-baseline leg of bench.py.  The oracle restates the reference's Julia
+algorithm for the LBM time step and its host preprocessing (see the headers
+of ol_oracle_kernels.cpp and ol_oracle_domain.cpp); parity against the
+reference itself is unpinned because the reference ships no tests, golden
+vectors or fixtures and its Julia toolchain is absent here.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB_PATH = HERE / "_build" / "libolorc.so"
+
+_lib = None
+
+
+def build(force: bool = False) -> Path:
+    """Compile the oracle with its Makefile (g++, -ffp-contract=off, OpenMP)."""
+    srcs = [HERE / "ol_oracle_kernels.cpp", HERE / "ol_oracle_domain.cpp", HERE / "Makefile"]
+    if force or not LIB_PATH.exists() or any(s.stat().st_mtime > LIB_PATH.stat().st_mtime for s in srcs):
+        r = subprocess.run(["make", "-C", str(HERE), "-B" if force else "all"],
+                           capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"oracle build failed:\n{r.stdout}\n{r.stderr}")
+    return LIB_PATH
+
+
+def lib() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            build()
+        _lib = C.CDLL(str(LIB_PATH))
+    return _lib
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+class StepParamsC(C.Structure):
+    from openludwig_b200._native import STEP_FIELDS as _f
+    _fields_ = _f
+
+
+class ThermalParamsC(C.Structure):
+    from openludwig_b200._native import THERMAL_FIELDS as _f
+    _fields_ = _f
+
+
+def _fill(struct_cls, d: dict):
+    s = struct_cls()
+    for name, _ in struct_cls._fields_:
+        if name in d:
+            setattr(s, name, d[name])
+    return s
+
+
+def stream_collide(lv: dict, pv: dict | None, params: dict, dtype=np.float32) -> None:
+    """One level sub-step in place on host arrays (see ol_stream_collide).
+    lv keys: f_out f_in f_post rho vel_out vel_in obstacle sponge wall_dist
+    neighbor_table map_x map_y map_z n_blocks; pv keys: f rho vel f_old
+    rho_old vel_old block_ptr dim n_blocks (or None on level 1)."""
+    fn = lib().orc_stream_collide_f32 if dtype == np.float32 else lib().orc_stream_collide_f64
+    sp = _fill(StepParamsC, params)
+    pv = pv or {}
+    dims = pv.get("dim", (0, 0, 0))
+    fn.restype = None
+    fn(_p(lv["f_out"]), _p(lv["f_in"]), _p(lv.get("f_post")), _p(lv["rho"]), _p(lv["vel_out"]),
+       _p(lv["vel_in"]), _p(lv["obstacle"]), _p(lv["sponge"]), _p(lv.get("wall_dist")),
+       _p(lv["neighbor_table"]), _p(lv["map_x"]), _p(lv["map_y"]), _p(lv["map_z"]),
+       C.c_int32(lv["n_blocks"]), _p(pv.get("f")), _p(pv.get("rho")), _p(pv.get("vel")),
+       _p(pv.get("f_old")), _p(pv.get("rho_old")), _p(pv.get("vel_old")),
+       _p(pv.get("block_ptr")), C.c_int32(dims[0]), C.c_int32(dims[1]), C.c_int32(dims[2]),
+       C.c_int32(pv.get("n_blocks", 0)), C.byref(sp))
+
+
+def bouzidi(f_out, f_post, q_map, cell_block, cx, cy, cz, neighbor_table, n_blocks, q_min,
+            dtype=np.float32) -> None:
+    fn = lib().orc_bouzidi_f32 if dtype == np.float32 else lib().orc_bouzidi_f64
+    fn.restype = None
+    fn(_p(f_out), _p(f_post), _p(q_map), _p(cell_block), _p(cx), _p(cy), _p(cz),
+       C.c_int32(len(cell_block)), _p(neighbor_table), C.c_int32(n_blocks), C.c_float(q_min))
+
+
+def thermal(tv: dict, pv: dict | None, params: dict, dtype=np.float32) -> None:
+    fn = lib().orc_thermal_f32 if dtype == np.float32 else lib().orc_thermal_f64
+    tp = _fill(ThermalParamsC, params)
+    pv = pv or {}
+    dims = pv.get("dim", (0, 0, 0))
+    fn.restype = None
+    fn(_p(tv["g_out"]), _p(tv["g_in"]), _p(tv.get("g_post")), _p(tv["T"]), _p(tv["vel"]),
+       _p(tv["obstacle"]), _p(tv["sponge"]), _p(tv["neighbor_table"]), _p(tv["map_x"]),
+       _p(tv["map_y"]), _p(tv["map_z"]), C.c_int32(tv["n_blocks"]), _p(pv.get("g")),
+       _p(pv.get("T")), _p(pv.get("vel")), _p(pv.get("g_old")), _p(pv.get("T_old")),
+       _p(pv.get("vel_old")), _p(pv.get("block_ptr")), C.c_int32(dims[0]), C.c_int32(dims[1]),
+       C.c_int32(dims[2]), C.c_int32(pv.get("n_blocks", 0)), C.byref(tp))
+
+
+# ------------------------------------------------------------------ domain
+
+def level_blocks(lvl, tris, dx, offset, dims, prev=None, prev_bs_phys=0.0, wake_box=None,
+                 margin_layers=2) -> np.ndarray:
+    t = np.ascontiguousarray(tris, dtype=np.float64)
+    off = np.ascontiguousarray(offset, dtype=np.float64)
+    pv = np.ascontiguousarray(prev if prev is not None else np.zeros((0, 3)), dtype=np.int32)
+    wb = np.ascontiguousarray(wake_box if wake_box is not None else np.zeros(6), dtype=np.float64)
+    cap = int(np.prod(dims)) if lvl == 1 else 1 << 20
+    while True:
+        out = np.zeros((cap, 3), dtype=np.int32)
+        fn = lib().orc_level_blocks
+        fn.restype = C.c_int
+        n = fn(C.c_int(lvl), _p(t), C.c_int(t.shape[0]), C.c_double(dx), _p(off), C.c_int(dims[0]),
+               C.c_int(dims[1]), C.c_int(dims[2]), _p(pv), C.c_int(pv.shape[0]),
+               C.c_double(prev_bs_phys), C.c_int(1 if wake_box is not None else 0), _p(wb),
+               C.c_int(margin_layers), _p(out), C.c_int(cap))
+        if n >= 0:
+            return out[:n].copy()
+        cap = -n
+
+
+def neighbor_table(coords, dims) -> np.ndarray:
+    c = np.ascontiguousarray(coords, dtype=np.int32)
+    out = np.zeros(27 * c.shape[0], dtype=np.int32)
+    lib().orc_neighbor_table(_p(c), C.c_int(c.shape[0]), C.c_int(dims[0]), C.c_int(dims[1]),
+                             C.c_int(dims[2]), _p(out))
+    return out
+
+
+def voxelize(coords, tris, dx, offset) -> np.ndarray:
+    c = np.ascontiguousarray(coords, dtype=np.int32)
+    t = np.ascontiguousarray(tris, dtype=np.float64)
+    off = np.ascontiguousarray(offset, dtype=np.float64)
+    out = np.zeros(c.shape[0] * 512, dtype=np.uint8)
+    lib().orc_voxelize(_p(c), C.c_int(c.shape[0]), _p(t), C.c_int(t.shape[0]), C.c_double(dx),
+                       _p(off), _p(out))
+    return out
+
+
+def flood_fill(coords, dims, obstacle) -> np.ndarray:
+    c = np.ascontiguousarray(coords, dtype=np.int32)
+    o = np.ascontiguousarray(obstacle, dtype=np.uint8).copy()
+    lib().orc_flood_fill(_p(c), C.c_int(c.shape[0]), C.c_int(dims[0]), C.c_int(dims[1]),
+                         C.c_int(dims[2]), _p(o))
+    return o
+
+
+def sponge(coords, dx, domain_size, thickness, symmetric) -> np.ndarray:
+    c = np.ascontiguousarray(coords, dtype=np.int32)
+    out = np.zeros(c.shape[0] * 512, dtype=np.float32)
+    lib().orc_sponge(_p(c), C.c_int(c.shape[0]), C.c_double(dx), C.c_double(domain_size[0]),
+                     C.c_double(domain_size[1]), C.c_double(domain_size[2]),
+                     C.c_float(thickness), C.c_int(1 if symmetric else 0), _p(out))
+    return out
+
+
+def wall_dist(coords, obstacle, dx) -> np.ndarray:
+    c = np.ascontiguousarray(coords, dtype=np.int32)
+    o = np.ascontiguousarray(obstacle, dtype=np.uint8)
+    out = np.full(c.shape[0] * 512, 100.0, dtype=np.float32)
+    lib().orc_wall_dist(_p(c), C.c_int(c.shape[0]), _p(o), C.c_double(dx), _p(out))
+    return out
+
+
+def bouzidi_qmap(coords, tris, dx, offset):
+    c = np.ascontiguousarray(coords, dtype=np.int32)
+    t = np.ascontiguousarray(tris, dtype=np.float64)
+    off = np.ascontiguousarray(offset, dtype=np.float64)
+    n = c.shape[0]
+    q = np.zeros(n * 512 * 27, dtype=np.uint16)
+    tri = np.zeros(n * 512 * 27, dtype=np.int32)
+    cap = n * 512
+    cells = np.zeros((max(cap, 1), 4), dtype=np.int32)
+    fn = lib().orc_bouzidi_qmap
+    fn.restype = C.c_int
+    cnt = fn(_p(c), C.c_int(n), _p(t), C.c_int(t.shape[0]), C.c_double(dx), _p(off), _p(q),
+             _p(tri), _p(cells), C.c_int(cap))
+    return q, tri, cells[:cnt].copy()
+
+
+def double_to_half_bits(x: float) -> int:
+    fn = lib().orc_double_to_half
+    fn.restype = C.c_uint16
+    return int(fn(C.c_double(x)))
+
+
+def half_to_float(h: int) -> float:
+    fn = lib().orc_half_to_float
+    fn.restype = C.c_float
+    return float(fn(C.c_uint16(h)))
+
+
+os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count() or 1))
