@@ -209,7 +209,8 @@ OL_API size_t ol_flow_stats_scratch_doubles(int32_t n_blocks);
 /* ------------------------------------------------------------------ */
 
 #define OL_STORE_F32 0
-#define OL_STORE_F16 1   /* f stored as binary16 of (f_k/w_k - 1) * scale */
+#define OL_STORE_F16 1   /* f stored as binary16 of (f_k - w_k) * scale / w_k */
+#define OL_STORE_DDF 2   /* flag: the pool also holds thermal populations     */
 
 typedef struct ol_ctx ol_ctx;
 
@@ -247,8 +248,12 @@ typedef struct ol_case_desc {
   float u_target;                           /* lattice inlet speed after ramp  */
   int32_t ramp_steps;                       /* cosine ramp (main.jl:217)       */
   int32_t async_depth;                      /* ramp batching (main.jl:210-218) */
+  float q_min_threshold;                    /* Bouzidi q threshold             */
+  float T_initial;                          /* initial temperature (DDF)       */
 } ol_case_desc;
 
+/* store_kind = OL_STORE_F32 or OL_STORE_F16, optionally | OL_STORE_DDF.
+ * The block pool (hbm_budget_bytes * 15/16) is allocated here, once. */
 OL_API int ol_ctx_create(ol_ctx **out, int device, size_t hbm_budget_bytes,
                   int store_kind);
 OL_API int ol_ctx_destroy(ol_ctx *ctx);
@@ -269,7 +274,8 @@ OL_API int ol_ctx_case_download(ol_ctx *ctx, int32_t case_id, int32_t level,
 /* Coarse steps a case has done, and its device watchdog status. */
 OL_API int ol_ctx_case_info(ol_ctx *ctx, int32_t case_id, int64_t *coarse_steps,
                      int32_t *status);
-/* Launch-shape autotuning over persistent grid sizes; result is kept. */
+/* Launch-shape autotuning over persistent grid sizes; result is kept.
+ * Timing replays advance every resident case by 4 * (trials + 1) steps. */
 OL_API int ol_ctx_autotune(ol_ctx *ctx, int32_t trials);
 /* Bytes in use / budget / number of resident cases / kernel launches issued. */
 OL_API int ol_ctx_stats(ol_ctx *ctx, size_t *used, size_t *budget, int32_t *n_cases,

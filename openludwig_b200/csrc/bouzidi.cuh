@@ -24,6 +24,9 @@ struct BouzDev {
   int64_t block_offset, dstride;
   float q_min, scale, inv_scale;
   float *scratch;       // [n_boundary*27] gathered values (two-phase)
+  int32_t desc;         // batched: owning level descriptor (f = its f_out / g_out)
+  int32_t thermal;      // batched: correct the thermal populations instead
+  int64_t scratch_off;  // batched: first scratch slot of this list
 };
 
 __device__ __forceinline__ float half_bits_to_float(uint16_t h) {

@@ -7,20 +7,11 @@
 // fixed order by a single-CTA pass, so the result is bitwise reproducible
 // (the reference accumulates FP32 atomics in arbitrary order).
 #include "common.cuh"
-#include "lattice.cuh"
+#include "forces.cuh"
 
 namespace ol {
 
-struct ForceDev {
-  ol_surface_mesh mesh;
-  const float *rho, *vel;
-  const uint8_t *obstacle;
-  const int32_t *bptr;
-  int64_t block_offset, dstride;
-  ol_force_params fp;
-  float *p_map, *sx_map, *sy_map, *sz_map;
-  double *partials;
-};
+
 
 // get_cell_at_position (surface.jl:192-222); 1-based global cell -> index
 __device__ __forceinline__ bool cell_at(const ForceDev &D, int gx, int gy, int gz, size_t &ci) {

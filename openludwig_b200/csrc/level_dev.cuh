@@ -64,6 +64,18 @@ struct LevelDev {
 
   ol_step_params sp;
   int32_t *status;        // device watchdog word (may be null)
+  const uint32_t *halo_tab;  // staging table (stream_collide.cuh)
 };
+
+// One unit of batched work: block `block` of the level described by
+// descriptor `desc`.
+struct WorkItem {
+  int32_t desc;
+  int32_t block;
+};
+
+// Per-device staging table of the 3176 out-of-block pull sources of a block
+// (built once on first use; see stage_block).
+const uint32_t *halo_table_device();
 
 }  // namespace ol

@@ -1,50 +1,97 @@
 // Drop-in stream-collide launch: one CTA per 8^3 block, one thread per cell,
 // caller buffers in the reference layout (FP32 populations).
+#include <mutex>
+#include <vector>
+
 #include "common.cuh"
-#include "stream_collide.cuh"
+#include "pipe.cuh"
 
 namespace ol {
 
-// The neighbour-table row of the block is staged in shared memory; the
-// 27 pull sources of a cell then need no further table reads.  Blocks with
-// an absent neighbour first park their boundary pulls in `ghost`.
-constexpr int kGhostBytes = 27 * BCELLS * sizeof(float);
+// Packed staging entries: k | dir << 5 | source cell << 10 | E slot << 19,
+// sorted by direction so consecutive threads read consecutive sources.
+static std::vector<uint32_t> build_halo_table() {
+  std::vector<uint32_t> tab;
+  for (int k = 0; k < 27; ++k)
+    for (int z = 0; z < 8; ++z)
+      for (int y = 0; y < 8; ++y)
+        for (int x = 0; x < 8; ++x) {
+          const int sx = x - cx_of(k), sy = y - cy_of(k), sz = z - cz_of(k);
+          if (sx >= 0 && sx < 8 && sy >= 0 && sy < 8 && sz >= 0 && sz < 8) continue;
+          const int ox = sx < 0 ? -1 : (sx > 7 ? 1 : 0);
+          const int oy = sy < 0 ? -1 : (sy > 7 ? 1 : 0);
+          const int oz = sz < 0 ? -1 : (sz > 7 ? 1 : 0);
+          const uint32_t dir = (ox + 1) + 3 * (oy + 1) + 9 * (oz + 1);
+          const uint32_t src = (sx & 7) + 8 * (sy & 7) + 64 * (sz & 7);
+          const uint32_t dst = e_index(sx, sy, sz);
+          tab.push_back((uint32_t)k | dir << 5 | src << 10 | dst << 19);
+        }
+  return tab;
+}
 
-// Cumulant fits 64 registers (2 CTAs of 512 threads per SM); the
-// regularized-BGK body keeps 27 equilibria in flight and gets 128.
+const uint32_t *halo_table_device() {
+  static std::mutex mu;
+  static uint32_t *per_dev[64] = {};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
+  std::lock_guard<std::mutex> lk(mu);
+  if (!per_dev[dev]) {
+    const std::vector<uint32_t> tab = build_halo_table();
+    if ((int)tab.size() != kHaloEntries) return nullptr;
+    uint32_t *d = nullptr;
+    if (cudaMalloc(&d, tab.size() * sizeof(uint32_t)) != cudaSuccess) return nullptr;
+    if (cudaMemcpy(d, tab.data(), tab.size() * sizeof(uint32_t), cudaMemcpyHostToDevice) !=
+        cudaSuccess) {
+      cudaFree(d);
+      return nullptr;
+    }
+    per_dev[dev] = d;
+  }
+  return per_dev[dev];
+}
+
+// One CTA per block: neighbour offsets, then the staged pull windows, then
+// the cell update.  Cumulant fits 64 registers (2 CTAs of 512 threads per
+// SM, 2 x 105 KB of staging); regularized BGK keeps 27 equilibria in flight
+// and gets 128.
 template <int OP, class ST, bool WALE>
 __global__ void __launch_bounds__(512, OP == OL_OP_CUMULANT ? 2 : 1)
     k_stream_collide(const __grid_constant__ LevelDev L) {
-  __shared__ int nb_blk[27];
-  __shared__ int n_missing;
-  extern __shared__ float ghost[];
+  __shared__ int nbbase[27];
+  extern __shared__ float E[];
   const int b = blockIdx.x;
-  if (threadIdx.x == 0) n_missing = 0;
+  load_nbbase(L.nbr, L.nbr_stride, L.block_offset, b, threadIdx.x, nbbase);
   __syncthreads();
-  if (threadIdx.x < 27) {
-    const int nb = L.nbr[b + L.nbr_stride * threadIdx.x];
-    nb_blk[threadIdx.x] = nb;
-    if (nb <= 0) atomicAdd(&n_missing, 1);
-  }
+  stage_flow<ST>(L, nbbase, b, threadIdx.x, E);
   __syncthreads();
-  if (n_missing) fill_ghost<ST>(L, nb_blk, b, threadIdx.x, ghost);
-  stream_collide_cell<OP, ST, WALE>(L, nb_blk, ghost, b, threadIdx.x);
-}
-
-template <int OP, class ST, bool WALE>
-static void set_smem_attr() {
-  static bool done = false;
-  if (!done) {
-    cudaFuncSetAttribute(k_stream_collide<OP, ST, WALE>,
-                         cudaFuncAttributeMaxDynamicSharedMemorySize, kGhostBytes);
-    done = true;
-  }
+  stream_collide_cell<OP, ST, WALE>(L, nbbase, E, b, threadIdx.x);
 }
 
 template <int OP, class ST, bool WALE>
 static void launch_one(const LevelDev &L, cudaStream_t s) {
-  set_smem_attr<OP, ST, WALE>();
-  k_stream_collide<OP, ST, WALE><<<L.n_blocks, BCELLS, kGhostBytes, s>>>(L);
+  static bool done = false;
+  if (!done) {
+    cudaFuncSetAttribute(k_stream_collide<OP, ST, WALE>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize, kStageBytes);
+    done = true;
+  }
+  k_stream_collide<OP, ST, WALE><<<L.n_blocks, BCELLS, kStageBytes, s>>>(L);
+}
+
+template <int OP, bool WALE>
+static void launch_pipe(const LevelDev &L, cudaStream_t s) {
+  static bool done = false;
+  static int n_sm = 148;
+  if (!done) {
+    cudaFuncSetAttribute(k_sc_pipe<OP, WALE, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         kPipeBytes);
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
+    done = true;
+  }
+  const int grid = L.n_blocks < n_sm ? L.n_blocks : n_sm;
+  k_sc_pipe<OP, WALE, false><<<grid, BCELLS, kPipeBytes, s>>>(L, nullptr, nullptr, 0);
 }
 
 template <class ST>
@@ -61,8 +108,18 @@ static void launch_sc(const LevelDev &L, cudaStream_t s) {
 
 void launch_stream_collide(const LevelDev &L, bool f16, cudaStream_t s) {
   if (L.n_blocks <= 0) return;
-  if (f16) launch_sc<StoreF16S>(L, s);
-  else launch_sc<StoreF32>(L, s);
+  if (f16) {
+    launch_sc<StoreF16S>(L, s);
+  } else {
+    const bool wale = L.sp.c_wale != 0.0f;
+    if (L.sp.op == OL_OP_CUMULANT) {
+      if (wale) launch_pipe<OL_OP_CUMULANT, true>(L, s);
+      else launch_pipe<OL_OP_CUMULANT, false>(L, s);
+    } else {
+      if (wale) launch_pipe<OL_OP_REGULARIZED_BGK, true>(L, s);
+      else launch_pipe<OL_OP_REGULARIZED_BGK, false>(L, s);
+    }
+  }
 }
 
 // f = f_temp = w_k; optional f_old = w_k, rho_old = 1, vel_old = 0 (main.jl:113-128)
@@ -114,6 +171,10 @@ extern "C" int ol_stream_collide(const ol_level_view *lv, const ol_parent_view *
   L.nbr_stride = lv->n_blocks;
   L.scale = 1.0f; L.inv_scale = 1.0f; L.p_inv_scale = 1.0f;
   L.sp = *sp;
+  OL_CHECK_ARG((int64_t)lv->n_blocks * BCELLS < (1LL << 31),
+               "ol_stream_collide: n_blocks too large for 32-bit plane offsets");
+  L.halo_tab = halo_table_device();
+  if (!L.halo_tab) return set_error(OL_ERR_CUDA, "ol_stream_collide: staging table allocation failed");
   if (!sp->is_level_1) {
     OL_CHECK_ARG(pv && pv->f && pv->rho && pv->vel && pv->block_ptr && pv->n_blocks > 0,
                  "ol_stream_collide: fine level needs a parent view");

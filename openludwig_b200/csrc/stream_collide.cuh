@@ -3,10 +3,11 @@
 // kernel_regularized_bgk.jl:43-325 in the same order:
 //   pull + domain BCs -> obstacle bounce-back -> rho, u, sponge -> wall
 //   model -> store u, rho -> WALE -> collision -> Guo forcing + store.
-// Rare paths (domain boundaries, level interfaces) run in a pre-phase that
-// parks their values in shared memory, so the bulk path has no call sites
-// and no address-taken arrays; the 27-direction loops are fully unrolled so
-// every lattice constant folds.
+// The block's pull windows are staged in shared memory first (stage_block),
+// rare paths (domain boundaries, level interfaces) fill their slots during
+// that staging, and the per-cell path has no call sites and no
+// address-taken arrays; the 27-direction loops are fully unrolled so every
+// lattice constant folds.
 #pragma once
 #include "level_dev.cuh"
 
@@ -139,38 +140,37 @@ __device__ __noinline__ float pull_boundary(const LevelDev &L, int k, int b,
 // WALE eddy viscosity from vel_in central differences
 // (kernel_cumulant.jl:264-305, physics_utils.jl:85-123).
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ void vel_neighbor(const LevelDev &L, const int *nb_blk,
-                                             int b, int x, int y, int z, int dx,
+__device__ __forceinline__ void vel_neighbor(const LevelDev &L, const int *nbbase,
+                                             int x, int y, int z, int dx,
                                              int dy, int dz, float &ux, float &uy,
                                              float &uz) {
   int nx = x + dx, ny = y + dy, nz = z + dz;
   const int ox = nx < 0 ? -1 : (nx > 7 ? 1 : 0);
   const int oy = ny < 0 ? -1 : (ny > 7 ? 1 : 0);
   const int oz = nz < 0 ? -1 : (nz > 7 ? 1 : 0);
-  const int nb = nb_blk[(ox + 1) + 3 * (oy + 1) + 9 * (oz + 1)];
+  const int nb = nbbase[(ox + 1) + 3 * (oy + 1) + 9 * (oz + 1)];
   size_t ci;
-  if (nb > 0) {
-    ci = (size_t)(L.block_offset + nb - 1) * BCELLS + (nx & 7) + BS * (ny & 7) +
-         BS * BS * (nz & 7);
+  if (nb >= 0) {
+    ci = (size_t)nb + (nx & 7) + BS * (ny & 7) + BS * BS * (nz & 7);
   } else {
-    ci = (size_t)(L.block_offset + b) * BCELLS + x + BS * y + BS * BS * z;
+    ci = (size_t)nbbase[13] + x + BS * y + BS * BS * z;
   }
   ux = __ldg(L.vel_in + ci);
   uy = __ldg(L.vel_in + ci + L.dstride);
   uz = __ldg(L.vel_in + ci + 2 * L.dstride);
 }
 
-__device__ __forceinline__ float wale_nu(const LevelDev &L, const int *nb_blk, int b,
-                                         int x, int y, int z) {
+__device__ __forceinline__ float wale_nu(const LevelDev &L, const int *nbbase, int x, int y,
+                                         int z) {
   float exx, eyx, ezx, wxx, wyx, wzx;  // E (x+1), W (x-1)
   float nxx, nyx, nzx, sxx, syx, szx;  // N (y+1), S (y-1)
   float txx, tyx, tzx, bxx, byx, bzx;  // T (z+1), B (z-1)
-  vel_neighbor(L, nb_blk, b, x, y, z, 1, 0, 0, exx, eyx, ezx);
-  vel_neighbor(L, nb_blk, b, x, y, z, -1, 0, 0, wxx, wyx, wzx);
-  vel_neighbor(L, nb_blk, b, x, y, z, 0, 1, 0, nxx, nyx, nzx);
-  vel_neighbor(L, nb_blk, b, x, y, z, 0, -1, 0, sxx, syx, szx);
-  vel_neighbor(L, nb_blk, b, x, y, z, 0, 0, 1, txx, tyx, tzx);
-  vel_neighbor(L, nb_blk, b, x, y, z, 0, 0, -1, bxx, byx, bzx);
+  vel_neighbor(L, nbbase, x, y, z, 1, 0, 0, exx, eyx, ezx);
+  vel_neighbor(L, nbbase, x, y, z, -1, 0, 0, wxx, wyx, wzx);
+  vel_neighbor(L, nbbase, x, y, z, 0, 1, 0, nxx, nyx, nzx);
+  vel_neighbor(L, nbbase, x, y, z, 0, -1, 0, sxx, syx, szx);
+  vel_neighbor(L, nbbase, x, y, z, 0, 0, 1, txx, tyx, tzx);
+  vel_neighbor(L, nbbase, x, y, z, 0, 0, -1, bxx, byx, bzx);
   const float g11 = 0.5f * (exx - wxx), g12 = 0.5f * (nxx - sxx), g13 = 0.5f * (txx - bxx);
   const float g21 = 0.5f * (eyx - wyx), g22 = 0.5f * (nyx - syx), g23 = 0.5f * (tyx - byx);
   const float g31 = 0.5f * (ezx - wzx), g32 = 0.5f * (nzx - szx), g33 = 0.5f * (tzx - bzx);
@@ -385,51 +385,115 @@ __device__ __forceinline__ void positivity_limit(float (&A)[27], float rho, floa
 // One cell of one block.  OP = OL_OP_*; WALE = gradients evaluated (c_wale
 // != 0; with c_wale == 0 the reference's nu_eddy is exactly 0).
 // ---------------------------------------------------------------------------
-// Boundary pre-phase: every pull of this cell whose source block is absent
-// gets its value (inlet/outlet equilibrium, free-slip mirror, parent
-// interpolation) written to its own shared-memory slot ghost[k*512 + t]
-// before the bulk pull runs, so the bulk path holds no call sites.
-template <class ST>
-__device__ __forceinline__ void fill_ghost(const LevelDev &L, const int *nb_blk, int b,
-                                           int t, float *ghost) {
-  const int x = t & 7, y = (t >> 3) & 7, z = t >> 6;
+// ---------------------------------------------------------------------------
+// Shared-memory staging of a block's 27 pull windows.
+//
+// E holds one halo-extended 10^3 plane per direction (E[k*1000 + (x+1) +
+// 10(y+1) + 100(z+1)] for x, y, z in -1..8), so the pull of cell (x, y, z)
+// in direction k is a single shared load at a compile-time offset from the
+// cell's base.  The own block's 27 planes are copied with 16-byte loads; the
+// 3176 out-of-block sources of the block (the slab each direction needs
+// from its up to 7 neighbours) come from a per-device table of packed
+// (k, neighbour direction, source cell, destination slot) entries; sources
+// whose neighbour block is absent get their boundary value (inlet/outlet
+// equilibrium, free-slip mirror, parent interpolation) right there.
+// nbbase[dir] = element offset of neighbour `dir` within a direction plane,
+// or -1 when it is absent.
+// ---------------------------------------------------------------------------
+constexpr int EPL = 1000;                 // floats per staged direction plane
+constexpr int kStageBytes = 27 * EPL * 4;  // dynamic shared memory per CTA
+constexpr int kHaloEntries = 3176;
+
+__host__ __device__ constexpr int e_index(int x, int y, int z) {
+  return (x + 1) + 10 * (y + 1) + 100 * (z + 1);
+}
+
+template <class ST, class BC>
+__device__ __forceinline__ void stage_block(const void *f_in_v, int64_t dstride, float inv_scale,
+                                            const int *nbbase, int t, float *E,
+                                            const uint32_t *__restrict__ tab, BC bc) {
+  using T = typename ST::T;
+  const T *__restrict__ fin = (const T *)f_in_v;
+  const int own = nbbase[13];
+  if (ST::kBytes == 4) {
+    const int c0 = (t & 127) * 4;
+    const int dst = e_index(c0 & 7, (c0 >> 3) & 7, c0 >> 6);
+#pragma unroll
+    for (int j = 0; j < 7; ++j) {
+      const int k = (t >> 7) + 4 * j;
+      if (k < 27) {
+        const float4 v = __ldg((const float4 *)((const float *)fin + (size_t)k * dstride + own + c0));
+        float *e = E + k * EPL + dst;
+        e[0] = v.x; e[1] = v.y; e[2] = v.z; e[3] = v.w;
+      }
+    }
+  } else {
+    const int c0 = (t & 63) * 8;
+    const int dst = e_index(0, (c0 >> 3) & 7, c0 >> 6);
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int k = (t >> 6) + 8 * j;
+      if (k < 27) {
+        const uint4 raw = __ldg((const uint4 *)((const __half *)fin + (size_t)k * dstride + own + c0));
+        const __half2 *h = (const __half2 *)&raw;
+        const float w = w_of(k), sc = w * inv_scale;
+        float *e = E + k * EPL + dst;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          const float2 f2 = __half22float2(h[i]);
+          e[2 * i] = fmaf(f2.x, sc, w);
+          e[2 * i + 1] = fmaf(f2.y, sc, w);
+        }
+      }
+    }
+  }
 #pragma unroll 1
-  for (int k = 0; k < 27; ++k) {
-    const int sx = x - cx_of(k), sy = y - cy_of(k), sz = z - cz_of(k);
-    const int ox = sx < 0 ? -1 : (sx > 7 ? 1 : 0);
-    const int oy = sy < 0 ? -1 : (sy > 7 ? 1 : 0);
-    const int oz = sz < 0 ? -1 : (sz > 7 ? 1 : 0);
-    if (nb_blk[(ox + 1) + 3 * (oy + 1) + 9 * (oz + 1)] <= 0)
-      ghost[k * BCELLS + t] = pull_boundary<ST>(L, k, b, x, y, z);
+  for (int i = t; i < kHaloEntries; i += BCELLS) {
+    const uint32_t te = __ldg(tab + i);
+    const int k = te & 31, dir = (te >> 5) & 31, src = (te >> 10) & 511, dst = te >> 19;
+    const int nb = nbbase[dir];
+    float v;
+    if (nb >= 0) {
+      v = ST::load(fin, (size_t)k * dstride + nb + src, k, inv_scale);
+    } else {
+      const int sx = dst % 10 - 1, sy = (dst / 10) % 10 - 1, sz = dst / 100 - 1;
+      v = bc(k, sx + cx_of(k), sy + cy_of(k), sz + cz_of(k));
+    }
+    E[k * EPL + dst] = v;
   }
 }
 
+// Neighbour-table row -> element offsets of the 27 neighbour blocks.
+__device__ __forceinline__ void load_nbbase(const int32_t *nbr, int64_t nbr_stride,
+                                            int64_t block_offset, int b, int t, int *nbbase) {
+  if (t < 27) {
+    const int nb = nbr[b + nbr_stride * t];
+    nbbase[t] = nb > 0 ? (int)((block_offset + nb - 1) * BCELLS) : -1;
+  }
+}
+
+// Stage the flow populations of block b of level L.
+template <class ST>
+__device__ __forceinline__ void stage_flow(const LevelDev &L, const int *nbbase, int b, int t,
+                                           float *E) {
+  stage_block<ST>(L.f_in, L.dstride, L.inv_scale, nbbase, t, E, L.halo_tab,
+                  [&](int k, int x, int y, int z) { return pull_boundary<ST>(L, k, b, x, y, z); });
+}
+
 template <int OP, class ST, bool WALE>
-__device__ __forceinline__ void stream_collide_cell(const LevelDev &L, const int *nb_blk,
-                                                    const float *ghost, int b, int t) {
+__device__ __forceinline__ void stream_collide_cell(const LevelDev &L, const int *nbbase,
+                                                    const float *E, int b, int t) {
   using T = typename ST::T;
   const int x = t & 7, y = (t >> 3) & 7, z = t >> 6;
   const ol_step_params &sp = L.sp;
-  const size_t own = (size_t)(L.block_offset + b) * BCELLS + t;
-  const T *__restrict__ fin = (const T *)L.f_in;
+  const size_t own = (size_t)nbbase[13] + t;
   T *__restrict__ fout = (T *)L.f_out;
 
   float A[27];
+  const int eb = e_index(x, y, z);
 #pragma unroll
-  for (int k = 0; k < 27; ++k) {
-    const int sx = x - cx_of(k), sy = y - cy_of(k), sz = z - cz_of(k);
-    const int ox = sx < 0 ? -1 : (sx > 7 ? 1 : 0);
-    const int oy = sy < 0 ? -1 : (sy > 7 ? 1 : 0);
-    const int oz = sz < 0 ? -1 : (sz > 7 ? 1 : 0);
-    const int nb = nb_blk[(ox + 1) + 3 * (oy + 1) + 9 * (oz + 1)];
-    const int local = (sx & 7) + BS * (sy & 7) + BS * BS * (sz & 7);
-    if (nb > 0)
-      A[k] = ST::load(fin, (size_t)(L.block_offset + nb - 1) * BCELLS + local +
-                               (size_t)k * L.dstride,
-                      k, L.inv_scale);
-    else
-      A[k] = ghost[k * BCELLS + t];
-  }
+  for (int k = 0; k < 27; ++k)
+    A[k] = E[k * EPL + eb - (cx_of(k) + 10 * cy_of(k) + 100 * cz_of(k))];
   float rho = 0.0f, jx = 0.0f, jy = 0.0f, jz = 0.0f;
 #pragma unroll
   for (int k = 0; k < 27; ++k) {
@@ -439,6 +503,10 @@ __device__ __forceinline__ void stream_collide_cell(const LevelDev &L, const int
     if (cz_of(k) == 1) jz += A[k]; else if (cz_of(k) == -1) jz -= A[k];
   }
   // Note: jx += v*cx in the reference equals jx +/- v exactly for cx = +/-1.
+  if (L.status) {  // device watchdog (native path): report, never trap
+    if (!(fabsf(rho) < 1e30f)) atomicOr(L.status, 1);
+    else if (rho < 0.01f) atomicOr(L.status, 2);
+  }
 
   float *fpost = (sp.store_post_collision && L.f_post) ? L.f_post : nullptr;
   if (L.obstacle[own]) {
@@ -485,7 +553,7 @@ __device__ __forceinline__ void stream_collide_cell(const LevelDev &L, const int
   L.rho_out[own] = rho;
 
   float nu_eddy = 0.0f;
-  if (WALE) nu_eddy = wale_nu(L, nb_blk, b, x, y, z);
+  if (WALE) nu_eddy = wale_nu(L, nbbase, x, y, z);
   nu_eddy = fmaxf(nu_eddy, sp.nu_sgs_background);
 
   float omega;  // omega_1 (cumulant) or omega (BGK)

@@ -4,35 +4,26 @@
 
 namespace ol {
 
-constexpr int kGhostBytesT = 27 * BCELLS * sizeof(float);
-
 template <class ST>
 __global__ void __launch_bounds__(512, 2) k_thermal(const __grid_constant__ ThermalDev D) {
-  __shared__ int nb_blk[27];
-  __shared__ int n_missing;
-  extern __shared__ float ghost[];
+  __shared__ int nbbase[27];
+  extern __shared__ float E[];
   const int b = blockIdx.x;
-  if (threadIdx.x == 0) n_missing = 0;
+  load_nbbase(D.nbr, D.nbr_stride, D.block_offset, b, threadIdx.x, nbbase);
   __syncthreads();
-  if (threadIdx.x < 27) {
-    const int nb = D.nbr[b + D.nbr_stride * threadIdx.x];
-    nb_blk[threadIdx.x] = nb;
-    if (nb <= 0) atomicAdd(&n_missing, 1);
-  }
+  stage_thermal<ST>(D, nbbase, b, threadIdx.x, E, D.halo_tab);
   __syncthreads();
-  if (n_missing) fill_ghost_thermal<ST>(D, nb_blk, b, threadIdx.x, ghost);
-  thermal_cell<ST>(D, nb_blk, ghost, b, threadIdx.x);
+  thermal_cell<ST>(D, nbbase, E, b, threadIdx.x);
 }
 
 template <class ST>
 static void launch_t(const ThermalDev &D, cudaStream_t s) {
   static bool done = false;
   if (!done) {
-    cudaFuncSetAttribute(k_thermal<ST>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         kGhostBytesT);
+    cudaFuncSetAttribute(k_thermal<ST>, cudaFuncAttributeMaxDynamicSharedMemorySize, kStageBytes);
     done = true;
   }
-  k_thermal<ST><<<D.n_blocks, BCELLS, kGhostBytesT, s>>>(D);
+  k_thermal<ST><<<D.n_blocks, BCELLS, kStageBytes, s>>>(D);
 }
 
 void launch_thermal(const ThermalDev &D, bool f16, cudaStream_t s) {
@@ -65,6 +56,8 @@ extern "C" int ol_thermal(const ol_thermal_view *tv, const ol_thermal_params *tp
   D.nbr_stride = tv->n_blocks;
   D.scale = 1.0f; D.inv_scale = 1.0f; D.p_inv_scale = 1.0f;
   D.tp = *tp;
+  D.halo_tab = halo_table_device();
+  if (!D.halo_tab) return set_error(OL_ERR_CUDA, "ol_thermal: staging table allocation failed");
   if (!tp->is_level_1) {
     OL_CHECK_ARG(tv->pg && tv->pT && tv->pvel && tv->p_block_ptr && tv->p_n_blocks > 0,
                  "ol_thermal: fine level needs parent thermal state");

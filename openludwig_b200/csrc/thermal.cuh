@@ -1,9 +1,9 @@
 // Thermal double-distribution stream-collide (kernel_thermal.jl:14-202):
 // passive-scalar BGK for 27 populations g driven by this sub-step's flow
-// velocity.  One CTA per block, one thread per cell, boundary pulls parked in
-// shared memory first as in the flow kernel.
+// velocity.  One CTA per block, one thread per cell, pull windows staged in
+// shared memory exactly as for the flow populations.
 #pragma once
-#include "level_dev.cuh"
+#include "stream_collide.cuh"
 
 namespace ol {
 
@@ -19,6 +19,7 @@ struct ThermalDev {
   int64_t p_block_offset, p_dstride;
   float p_inv_scale;
   ol_thermal_params tp;
+  const uint32_t *halo_tab;
 };
 
 // Coarse-to-fine thermal ghost (physics_interpolation.jl:135-247).
@@ -127,55 +128,38 @@ __device__ __noinline__ float pull_boundary_thermal(const ThermalDev &D, int k, 
   return w * tp.T_inlet;
 }
 
+// Stage the thermal populations of block b (same layout as the flow).
 template <class ST>
-__device__ __forceinline__ void fill_ghost_thermal(const ThermalDev &D, const int *nb_blk, int b,
-                                                   int t, float *ghost) {
-  const int x = t & 7, y = (t >> 3) & 7, z = t >> 6;
-#pragma unroll 1
-  for (int k = 0; k < 27; ++k) {
-    const int sx = x - cx_of(k), sy = y - cy_of(k), sz = z - cz_of(k);
-    const int ox = sx < 0 ? -1 : (sx > 7 ? 1 : 0);
-    const int oy = sy < 0 ? -1 : (sy > 7 ? 1 : 0);
-    const int oz = sz < 0 ? -1 : (sz > 7 ? 1 : 0);
-    if (nb_blk[(ox + 1) + 3 * (oy + 1) + 9 * (oz + 1)] <= 0)
-      ghost[k * BCELLS + t] = pull_boundary_thermal<ST>(D, k, b, x, y, z);
-  }
+__device__ __forceinline__ void stage_thermal(const ThermalDev &D, const int *nbbase, int b, int t,
+                                              float *E, const uint32_t *tab) {
+  stage_block<ST>(D.g_in, D.dstride, D.inv_scale, nbbase, t, E, tab,
+                  [&](int k, int x, int y, int z) {
+                    return pull_boundary_thermal<ST>(D, k, b, x, y, z);
+                  });
 }
 
 template <class ST>
-__device__ __forceinline__ void thermal_cell(const ThermalDev &D, const int *nb_blk,
-                                             const float *ghost, int b, int t) {
+__device__ __forceinline__ void thermal_cell(const ThermalDev &D, const int *nbbase,
+                                             const float *E, int b, int t) {
   using T = typename ST::T;
   const int x = t & 7, y = (t >> 3) & 7, z = t >> 6;
   const ol_thermal_params &tp = D.tp;
-  const size_t own = (size_t)(D.block_offset + b) * BCELLS + t;
-  const T *__restrict__ gin = (const T *)D.g_in;
+  const size_t own = (size_t)nbbase[13] + t;
   T *__restrict__ gout = (T *)D.g_out;
   float ux = D.vel[own], uy = D.vel[own + D.dstride], uz = D.vel[own + 2 * D.dstride];
+  const int eb = e_index(x, y, z);
   float G[27];
   float Tsum = 0.0f;
 #pragma unroll
   for (int k = 0; k < 27; ++k) {
-    const int sx = x - cx_of(k), sy = y - cy_of(k), sz = z - cz_of(k);
-    const int ox = sx < 0 ? -1 : (sx > 7 ? 1 : 0);
-    const int oy = sy < 0 ? -1 : (sy > 7 ? 1 : 0);
-    const int oz = sz < 0 ? -1 : (sz > 7 ? 1 : 0);
-    const int nb = nb_blk[(ox + 1) + 3 * (oy + 1) + 9 * (oz + 1)];
-    const int local = (sx & 7) + BS * (sy & 7) + BS * BS * (sz & 7);
-    if (nb > 0)
-      G[k] = ST::load(gin, (size_t)(D.block_offset + nb - 1) * BCELLS + local +
-                               (size_t)k * D.dstride,
-                      k, D.inv_scale);
-    else
-      G[k] = ghost[k * BCELLS + t];
+    G[k] = E[k * EPL + eb - (cx_of(k) + 10 * cy_of(k) + 100 * cz_of(k))];
     Tsum += G[k];
   }
   float *gpost = (tp.store_post_collision && D.g_post) ? D.g_post : nullptr;
   if (D.obstacle[own]) {
 #pragma unroll
     for (int k = 0; k < 27; ++k) {
-      const int ko = opp_of(k);
-      const float gopp = ST::load(gin, own + (size_t)ko * D.dstride, ko, D.inv_scale);
+      const float gopp = E[opp_of(k) * EPL + eb];  // g_in at this cell, opposite link
       float v;
       if (tp.wall_bc_adiabatic == 1) {
         v = gopp;

@@ -337,3 +337,130 @@ def cells_total(levels) -> int:
 def cell_updates_per_coarse_step(levels) -> int:
     """True cell updates: level l advances 2^(l-1) times per coarse step."""
     return sum(lv.n_blocks * 512 * (1 << i) for i, lv in enumerate(levels))
+
+
+# --------------------------------------------------------------------- forces
+
+@dc.dataclass
+class DeviceMesh:
+    """upload_mesh_to_gpu (geometry.jl:50-69): FP32 centres, normals, areas."""
+    arrays: torch.Tensor   # [7, n]: cx cy cz nx ny nz area
+    n: int
+
+    def view(self) -> N.SurfaceMesh:
+        a = self.arrays
+        return N.SurfaceMesh(cx=_ptr(a[0]), cy=_ptr(a[1]), cz=_ptr(a[2]), nx=_ptr(a[3]),
+                             ny=_ptr(a[4]), nz=_ptr(a[5]), area=_ptr(a[6]), n_triangles=self.n)
+
+
+def upload_mesh(mesh, device) -> DeviceMesh:
+    a = np.stack([mesh.centers[:, 0], mesh.centers[:, 1], mesh.centers[:, 2], mesh.normals[:, 0],
+                  mesh.normals[:, 1], mesh.normals[:, 2], mesh.areas]).astype(np.float32)
+    return DeviceMesh(torch.from_numpy(np.ascontiguousarray(a)).to(device), mesh.n)
+
+
+def force_params_for(lv: DeviceLevel, p: DomainParams, cfg: CaseConfig,
+                     search_radius: int = 5) -> N.ForceParams:
+    vs = p.velocity_scale
+    ps = float(np.float32(p.rho_physical * vs * vs))
+    h = lv.host
+    mc, off = p.moment_center, p.mesh_offset
+    return N.ForceParams(dx=float(np.float32(h.dx)), dim_x=h.grid_dim[0], dim_y=h.grid_dim[1],
+                         dim_z=h.grid_dim[2], offset_x=off[0], offset_y=off[1], offset_z=off[2],
+                         pressure_scale=ps, stress_scale=ps, tau_molecular=h.tau,
+                         search_radius=search_radius, c_wale=cfg.c_wale,
+                         nu_sgs_bg=cfg.nu_sgs_background, ref_x=mc[0], ref_y=mc[1], ref_z=mc[2])
+
+
+def compute_aerodynamics(lv: DeviceLevel, dmesh: DeviceMesh, p: DomainParams, cfg: CaseConfig,
+                         vel: torch.Tensor | None = None, maps: bool = False,
+                         search_radius: int = 5):
+    """compute_aerodynamics! (surface.jl:913-920) on a level: returns the raw
+    nine sums (and the per-triangle p / shear maps when maps=True).  `vel`
+    defaults to the level's `vel` buffer, as the reference reads `level.vel`."""
+    fp = force_params_for(lv, p, cfg, search_radius)
+    n = dmesh.n
+    dev = lv.rho.device
+    partials = torch.empty(int(N.lib().ol_surface_forces_scratch_doubles(n)), dtype=torch.float64,
+                           device=dev)
+    m = torch.empty((4, n), dtype=torch.float32, device=dev) if maps else None
+    out = (C.c_double * 9)()
+    N.call("ol_surface_forces", C.byref(dmesh.view()), _ptr(lv.rho), _ptr(vel if vel is not None else lv.vel),
+           _ptr(lv.obstacle), _ptr(lv.block_ptr), N.i32(lv.n_blocks), C.byref(fp),
+           _ptr(m[0]) if maps else None, _ptr(m[1]) if maps else None,
+           _ptr(m[2]) if maps else None, _ptr(m[3]) if maps else None, _ptr(partials), out,
+           _stream())
+    raw = np.array(out[:], dtype=np.float64)
+    return (raw, m) if maps else raw
+
+
+def flow_stats(lv: DeviceLevel) -> dict:
+    """compute_flow_stats (diagnostics.jl:43-93) in FP64."""
+    partials = torch.empty(int(N.lib().ol_flow_stats_scratch_doubles(lv.n_blocks)),
+                           dtype=torch.float64, device=lv.rho.device)
+    out = (C.c_double * 7)()
+    N.call("ol_flow_stats", _ptr(lv.rho), _ptr(lv.vel), _ptr(lv.obstacle), N.i32(lv.n_blocks),
+           _ptr(partials), out, _stream())
+    n = out[0]
+    return {"n_fluid": int(n), "rho_mean": out[1] / n if n else 1.0, "rho_min": out[2],
+            "rho_max": out[3], "v_max": out[4], "kinetic_energy": out[5], "mass": out[6]}
+
+
+class Simulation:
+    """main.jl solve_main() time loop over the device levels: batched cosine
+    inlet ramp, diagnostics every diag_freq steps, surface forces on the
+    finest level, time averaging after the ramp (ForceAccumulator)."""
+
+    def __init__(self, cfg: CaseConfig, mesh, p: DomainParams, hosts, device=None):
+        from .native import coefficients
+        self._coeff = coefficients
+        self.cfg, self.mesh, self.p = cfg, mesh, p
+        self.device = device or torch.device("cuda", torch.cuda.current_device())
+        self.levels = [upload_level(h, self.device, ddf=cfg.ddf_enabled, t_init=cfg.ddf_t_initial)
+                       for h in hosts]
+        self.settings = StepSettings.from_config(cfg, cfg.wall_model_enabled)
+        self.dmesh = upload_mesh(mesh, self.device)
+        self.dims = (p.nx_coarse, p.ny_coarse, p.nz_coarse)
+        self.t = 0
+        self.history: list[dict] = []
+        self.acc = np.zeros(9)
+        self.n_avg = 0
+
+    def forces(self):
+        raw = compute_aerodynamics(self.levels[-1], self.dmesh, self.p, self.cfg)
+        return self._coeff(raw, self.p.rho_physical, self.p.u_physical, self.p.reference_area,
+                           self.p.reference_chord, self.cfg.symmetric_analysis), raw
+
+    def run(self, steps: int, diag_freq: int | None = None) -> list[dict]:
+        cfg = self.cfg
+        diag = diag_freq or cfg.diag_freq
+        batch = max(1, cfg.async_depth)
+        end = self.t + steps
+        t = self.t + 1
+        while t <= end:
+            batch_end = min(t + batch - 1, end)
+            actual = batch_end - t + 1
+            u = ramp_velocity(cfg.u_target, batch_end, cfg.ramp_steps)
+            execute_timestep_batch(self.levels, self.settings, t, actual, u, self.dims)
+            if batch_end % diag < actual or batch_end == end:
+                d = (batch_end // diag) * diag
+                if t <= d <= batch_end:
+                    rec = {"step": d, "u": u, **flow_stats(self.levels[0])}
+                    if cfg.forces_enabled:
+                        fr, raw = self.forces()
+                        rec.update(Cd=fr.Cd, Cl=fr.Cl, Cs=fr.Cs, Cmy=fr.Cmy)
+                        if d > cfg.ramp_steps:
+                            self.acc += raw
+                            self.n_avg += 1
+                    self.history.append(rec)
+            t = batch_end + 1
+        self.t = end
+        return self.history
+
+    def averaged(self):
+        """print_averaged_summary (surface.jl:58-139) coefficients."""
+        if self.n_avg == 0:
+            return None
+        return self._coeff(self.acc / self.n_avg, self.p.rho_physical, self.p.u_physical,
+                           self.p.reference_area, self.p.reference_chord,
+                           self.cfg.symmetric_analysis)

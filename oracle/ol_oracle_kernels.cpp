@@ -723,6 +723,80 @@ void thermal(R *g_out, const R *g_in, R *g_post, R *T_out, const R *vel, const u
         }
 }
 
+
+// ---------------------------------------------------------------------------
+// Surface forces (surface.jl:143-507 map, 702-762 integrate), FP32 per
+// triangle.  The reference adds the per-triangle terms with FP32 atomics in
+// arbitrary order; here they are summed in FP64 in triangle order.
+// ---------------------------------------------------------------------------
+struct ForceP {
+  float dx; int32_t dim_x, dim_y, dim_z;
+  float off_x, off_y, off_z, pressure_scale, stress_scale, tau;
+  int32_t search_radius;
+  float c_wale, nu_bg, ref_x, ref_y, ref_z;
+};
+
+static bool cell_at(const int32_t *bptr, const ForceP &fp, int gx, int gy, int gz, size_t &ci) {
+  if (gx < 1 || gy < 1 || gz < 1) return false;
+  int bx = (gx - 1) / BS + 1, by = (gy - 1) / BS + 1, bz = (gz - 1) / BS + 1;
+  if (bx < 1 || bx > fp.dim_x || by < 1 || by > fp.dim_y || bz < 1 || bz > fp.dim_z) return false;
+  int b = bptr[(bx - 1) + fp.dim_x * ((by - 1) + fp.dim_y * (bz - 1))];
+  if (b <= 0) return false;
+  ci = (size_t)(b - 1) * NC + (gx - 1) % BS + BS * ((gy - 1) % BS) + BS * BS * ((gz - 1) % BS);
+  return true;
+}
+
+static bool trilinear(const float *rho, const float *vel, const uint8_t *obs, const int32_t *bptr,
+                      size_t S, const ForceP &fp, float px, float py, float pz, float &r, float &ux,
+                      float &uy, float &uz, float &wq) {
+  float inv = 1.0f / fp.dx;
+  float fx = px * inv - 0.5f, fy = py * inv - 0.5f, fz = pz * inv - 0.5f;
+  int ix0 = (int)std::floor(fx) + 1, iy0 = (int)std::floor(fy) + 1, iz0 = (int)std::floor(fz) + 1;
+  float wx = rclamp(fx - (float)(ix0 - 1), 0.0f, 1.0f);
+  float wy = rclamp(fy - (float)(iy0 - 1), 0.0f, 1.0f);
+  float wz = rclamp(fz - (float)(iz0 - 1), 0.0f, 1.0f);
+  float w0x = 1.0f - wx, w1x = wx, w0y = 1.0f - wy, w1y = wy, w0z = 1.0f - wz, w1z = wz;
+  float ra = 0, xa = 0, ya = 0, za = 0, wa = 0;
+  const int ox[8] = {0, 1, 0, 1, 0, 1, 0, 1}, oy[8] = {0, 0, 1, 1, 0, 0, 1, 1}, oz[8] = {0, 0, 0, 0, 1, 1, 1, 1};
+  for (int s = 0; s < 8; ++s) {
+    float w = (ox[s] ? w1x : w0x) * (oy[s] ? w1y : w0y) * (oz[s] ? w1z : w0z);
+    size_t ci;
+    if (cell_at(bptr, fp, ix0 + ox[s], iy0 + oy[s], iz0 + oz[s], ci) && !obs[ci]) {
+      ra += w * rho[ci];
+      xa += w * vel[ci];
+      ya += w * vel[ci + S];
+      za += w * vel[ci + 2 * S];
+      wa += w;
+    }
+  }
+  if (wa > 0.01f) {
+    float iw = 1.0f / wa;
+    r = ra * iw; ux = xa * iw; uy = ya * iw; uz = za * iw; wq = wa;
+    return true;
+  }
+  r = 1.0f; ux = uy = uz = 0.0f; wq = 0.0f;
+  return false;
+}
+
+static void stress(const ForceP &fp, float rho, float ux, float uy, float uz, float nx, float ny,
+                   float nz, float d, float &p, float &tx, float &ty, float &tz) {
+  p = (rho - 1.0f) / 3.0f * fp.pressure_scale;
+  float un = ux * nx + uy * ny + uz * nz;
+  float utx = ux - un * nx, uty = uy - un * ny, utz = uz - un * nz;
+  float ut = std::sqrt(utx * utx + uty * uty + utz * utz);
+  float nu_mol = (fp.tau - 0.5f) / 3.0f;
+  float nu_sgs = 0.0f;
+  if (fp.c_wale > 0.0f && d > 0.01f && ut > 1e-10f) nu_sgs = (fp.c_wale * fp.c_wale) * (ut / d);
+  nu_sgs = rmax(nu_sgs, fp.nu_bg);
+  float nu_eff = nu_mol + nu_sgs;
+  tx = ty = tz = 0.0f;
+  if (ut > 1e-10f && d > 0.01f) {
+    float tl = rho * nu_eff * ut / d;
+    float tph = tl * fp.stress_scale;
+    tx = (utx / ut) * tph; ty = (uty / ut) * tph; tz = (utz / ut) * tph;
+  }
+}
+
 }  // namespace orc
 
 using namespace orc;
@@ -772,5 +846,70 @@ void orc_bouzidi_f64(double *f_out, const double *f_post, const uint16_t *q, con
 void orc_thermal_f32(ORC_THERMAL_ARGS(float)) { ORC_THERMAL_BODY(float) }
 void orc_thermal_f64(ORC_THERMAL_ARGS(double)) { ORC_THERMAL_BODY(double) }
 
+
+void orc_surface_forces(const float *cx, const float *cy, const float *cz, const float *nx,
+                        const float *ny, const float *nz, const float *area, int32_t ntri,
+                        const float *rho, const float *vel, const uint8_t *obs,
+                        const int32_t *bptr, int32_t nB, const ForceP *fpp, float *pmap,
+                        float *sxm, float *sym, float *szm, double *out) {
+  const ForceP &fp = *fpp;
+  const size_t S = (size_t)NC * nB;
+  for (int j = 0; j < 9; ++j) out[j] = 0.0;
+  for (int i = 0; i < ntri; ++i) {
+    float tx = cx[i] + fp.off_x, ty = cy[i] + fp.off_y, tz = cz[i] + fp.off_z;
+    float n_x = nx[i], n_y = ny[i], n_z = nz[i];
+    float br = 1.0f, bux = 0, buy = 0, buz = 0, bd = 1.0f, bq = 0.0f;
+    bool found = false;
+    for (int pi = 1; pi <= fp.search_radius; ++pi) {
+      float dc = (float)pi + 0.5f;
+      float r, ux, uy, uz, wq;
+      bool ok = trilinear(rho, vel, obs, bptr, S, fp, tx + n_x * dc * fp.dx, ty + n_y * dc * fp.dx,
+                          tz + n_z * dc * fp.dx, r, ux, uy, uz, wq);
+      if (ok && wq >= 0.5f) { br = r; bux = ux; buy = uy; buz = uz; bd = dc; bq = wq; found = true; break; }
+      if (ok && wq > bq) { br = r; bux = ux; buy = uy; buz = uz; bd = dc; bq = wq; found = true; }
+    }
+    if (!found) {
+      int gx0 = (int)std::floor(tx / fp.dx) + 1, gy0 = (int)std::floor(ty / fp.dx) + 1,
+          gz0 = (int)std::floor(tz / fp.dx) + 1;
+      float best = 1e10f;
+      for (int rad = 1; rad <= fp.search_radius; ++rad) {
+        if (found) break;
+        for (int dz = -rad; dz <= rad; ++dz)
+          for (int dy = -rad; dy <= rad; ++dy)
+            for (int ddx = -rad; ddx <= rad; ++ddx) {
+              if (!(std::abs(ddx) == rad || std::abs(dy) == rad || std::abs(dz) == rad)) continue;
+              int gx = gx0 + ddx, gy = gy0 + dy, gz = gz0 + dz;
+              size_t ci;
+              if (!cell_at(bptr, fp, gx, gy, gz, ci) || obs[ci]) continue;
+              float ddxp = ((float)gx - 0.5f) * fp.dx - tx, ddyp = ((float)gy - 0.5f) * fp.dx - ty,
+                    ddzp = ((float)gz - 0.5f) * fp.dx - tz;
+              float dn = ddxp * n_x + ddyp * n_y + ddzp * n_z;
+              if (dn <= 0.0f) continue;
+              float d2 = ddxp * ddxp + ddyp * ddyp + ddzp * ddzp;
+              if (d2 < best) {
+                best = d2; br = rho[ci]; bux = vel[ci]; buy = vel[ci + S]; buz = vel[ci + 2 * S];
+                bd = dn / fp.dx; found = true;
+              }
+            }
+      }
+    }
+    float p = 0, sx = 0, sy = 0, sz = 0;
+    if (found) stress(fp, br, bux, buy, buz, n_x, n_y, n_z, rmax(bd, 0.5f), p, sx, sy, sz);
+    if (pmap) { pmap[i] = p; sxm[i] = sx; sym[i] = sy; szm[i] = sz; }
+    float A = area[i];
+    float fpx = -p * n_x * A, fpy = -p * n_y * A, fpz = -p * n_z * A;
+    float fvx = sx * A, fvy = sy * A, fvz = sz * A;
+    float Fx = fpx + fvx, Fy = fpy + fvy, Fz = fpz + fvz;
+    float rx = tx - fp.ref_x, ry = ty - fp.ref_y, rz = tz - fp.ref_z;
+    out[0] += fpx; out[1] += fpy; out[2] += fpz; out[3] += fvx; out[4] += fvy; out[5] += fvz;
+    out[6] += (double)(ry * Fz - rz * Fy);
+    out[7] += (double)(rz * Fx - rx * Fz);
+    out[8] += (double)(rx * Fy - ry * Fx);
+  }
+}
+
 float orc_half_to_float(uint16_t h) { return h2f(h); }
+float orc_gradient_noise(int32_t gx, int32_t gy, int32_t gz, int32_t seed) {
+  return gradient_noise(gx, gy, gz, seed);
+}
 }

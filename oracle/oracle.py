@@ -186,10 +186,36 @@ def bouzidi_qmap(coords, tris, dx, offset):
     return q, tri, cells[:cnt].copy()
 
 
+class ForceParamsC(C.Structure):
+    from openludwig_b200._native import ForceParams as _F
+    _fields_ = _F._fields_
+
+
+def surface_forces(mesh_arrays, rho, vel, obstacle, block_ptr, n_blocks, fp_struct):
+    """Per-triangle (p, tau_x, tau_y, tau_z) maps and the nine force/moment sums.
+    mesh_arrays: float32 [7, n] (cx cy cz nx ny nz area)."""
+    m = np.ascontiguousarray(mesh_arrays, dtype=np.float32)
+    n = m.shape[1]
+    maps = np.zeros((4, n), np.float32)
+    out = np.zeros(9, np.float64)
+    fp = ForceParamsC()
+    C.memmove(C.byref(fp), C.byref(fp_struct), C.sizeof(fp))
+    lib().orc_surface_forces(*[_p(m[i]) for i in range(7)], C.c_int32(n), _p(rho), _p(vel),
+                             _p(obstacle), _p(block_ptr), C.c_int32(n_blocks), C.byref(fp),
+                             _p(maps[0]), _p(maps[1]), _p(maps[2]), _p(maps[3]), _p(out))
+    return out, maps
+
+
 def double_to_half_bits(x: float) -> int:
     fn = lib().orc_double_to_half
     fn.restype = C.c_uint16
     return int(fn(C.c_double(x)))
+
+
+def gradient_noise(gx: int, gy: int, gz: int, seed: int) -> float:
+    fn = lib().orc_gradient_noise
+    fn.restype = C.c_float
+    return float(fn(C.c_int32(gx), C.c_int32(gy), C.c_int32(gz), C.c_int32(seed)))
 
 
 def half_to_float(h: int) -> float:
