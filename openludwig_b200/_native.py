@@ -14,7 +14,7 @@ OL_OK = 0
 OL_OP_CUMULANT = 0
 OL_OP_REGULARIZED_BGK = 1
 OL_LIMITER_NONE, OL_LIMITER_FACTORED, OL_LIMITER_POSITIVITY = 0, 1, 2
-OL_STORE_F32, OL_STORE_F16 = 0, 1
+OL_STORE_F32, OL_STORE_F16, OL_STORE_DDF = 0, 1, 2
 
 vp = C.c_void_p
 i32 = C.c_int32
@@ -98,7 +98,7 @@ class CaseDesc(C.Structure):
                 ("n_triangles", i32), ("tri_cx", vp), ("tri_cy", vp), ("tri_cz", vp),
                 ("tri_nx", vp), ("tri_ny", vp), ("tri_nz", vp), ("tri_area", vp),
                 ("force", ForceParams), ("u_target", f32), ("ramp_steps", i32),
-                ("async_depth", i32)]
+                ("async_depth", i32), ("q_min_threshold", f32), ("T_initial", f32)]
 
 
 class OLError(RuntimeError):
