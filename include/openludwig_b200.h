@@ -131,6 +131,25 @@ OL_API int ol_bouzidi_sparse(float *f_out, const uint16_t *q_map,
                       int32_t n_blocks, float q_min_threshold, float *scratch,
                       void *stream);
 
+/* Same correction as ol_bouzidi_sparse for callers that cannot allocate
+ * device memory: callers whose memory is held by another allocator's pool
+ * (CUDA.jl, PyTorch caching allocators) or loops that must not allocate.
+ * No counterpart in the reference (it always allocates f_post_collision).
+ * The scratch is a fixed library-owned device array sized for
+ * OL_BOUZIDI_NOALLOC_MAX_CELLS boundary cells (27 floats each, 7 MB, held by
+ * every device that loads the library until exit); larger n_boundary is
+ * rejected with OL_ERR_ARG.  The call allocates nothing.  Its first call on
+ * a device looks up the array's device address (once per device, that
+ * device current); make that first call before any stream capture.  All
+ * calls share the one array: calls that overlap on the GPU (other streams,
+ * other host threads) race on it. */
+#define OL_BOUZIDI_NOALLOC_MAX_CELLS 65536
+OL_API int ol_bouzidi_sparse_noalloc(float *f_out, const uint16_t *q_map,
+                      const int32_t *cell_block, const int8_t *cell_x,
+                      const int8_t *cell_y, const int8_t *cell_z,
+                      int32_t n_boundary, const int32_t *neighbor_table,
+                      int32_t n_blocks, float q_min_threshold, void *stream);
+
 /* Thermal DDF level view + parameters (kernel_thermal.jl:14-40). */
 typedef struct ol_thermal_view {
   float *g_out; const float *g_in; float *g_post;  /* g_post may be NULL     */

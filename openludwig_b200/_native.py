@@ -117,6 +117,7 @@ _SIGS = {
                                     C.POINTER(StepParams), vp]),
     "ol_bouzidi": (C.c_int, [vp, vp, vp, vp, vp, vp, vp, i32, vp, i32, f32, vp]),
     "ol_bouzidi_sparse": (C.c_int, [vp, vp, vp, vp, vp, vp, i32, vp, i32, f32, vp, vp]),
+    "ol_bouzidi_sparse_noalloc": (C.c_int, [vp, vp, vp, vp, vp, vp, i32, vp, i32, f32, vp]),
     "ol_thermal": (C.c_int, [C.POINTER(ThermalView), C.POINTER(ThermalParams), vp]),
     "ol_init_equilibrium": (C.c_int, [vp, vp, vp, vp, vp, i32, vp]),
     "ol_surface_forces": (C.c_int, [C.POINTER(SurfaceMesh), vp, vp, vp, vp, i32,
