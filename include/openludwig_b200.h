@@ -72,8 +72,18 @@ typedef struct ol_level_view {
   const float *wall_dist;       /* [512*nB]    may be NULL if no wall model    */
   const int32_t *neighbor_table;/* [nB*27]     1-based ids, 0 = missing        */
   const int32_t *map_x, *map_y, *map_z; /* [nB] 1-based block coordinates     */
+  float *ghost;                 /* [ol_ghost_floats(nB)] scratch, or NULL (below) */
   int32_t n_blocks;
 } ol_level_view;
+
+/* Size (floats) of the optional ol_level_view.ghost scratch.  No reference
+ * counterpart: with ghost set, ol_stream_collide first evaluates, in a
+ * separate pass over the blocks that have an absent neighbour, the boundary
+ * values those pulls read (inlet/outlet equilibria, free-slip mirrors,
+ * coarse-to-fine interpolation; kernel_cumulant.jl:117-159), then streams
+ * them like neighbour data.  With ghost NULL the same values are computed
+ * while the block is staged.  Results are identical either way. */
+OL_API int64_t ol_ghost_floats(int32_t n_blocks);
 
 /* Parent-level state for coarse-to-fine ghost interpolation
  * (physics_interpolation.jl:4-127).  Ignored when is_level_1 != 0. */
@@ -284,6 +294,9 @@ OL_API int ol_ctx_case_remove(ol_ctx *ctx, int32_t case_id);
  * per coarse step).  Asynchronous on the context stream. */
 OL_API int ol_ctx_step(ol_ctx *ctx, int32_t n_coarse);
 OL_API int ol_ctx_sync(ol_ctx *ctx);
+/* ol_ctx_step followed by a synchronize, timed with CUDA events recorded on
+ * the context stream around the replays; *ms = device time of the n steps. */
+OL_API int ol_ctx_step_timed(ol_ctx *ctx, int32_t n_coarse, float *ms);
 /* Surface forces of one case on its finest level: out[9] as ol_surface_forces. */
 OL_API int ol_ctx_case_forces(ol_ctx *ctx, int32_t case_id, double out[9]);
 /* Download a level's macroscopic fields (host buffers of 512*nB / 512*nB*3),

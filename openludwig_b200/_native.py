@@ -25,7 +25,7 @@ class LevelView(C.Structure):
     _fields_ = [("f_out", vp), ("f_in", vp), ("f_post", vp), ("rho", vp), ("vel_out", vp),
                 ("vel_in", vp), ("obstacle", vp), ("sponge", vp), ("wall_dist", vp),
                 ("neighbor_table", vp), ("map_x", vp), ("map_y", vp), ("map_z", vp),
-                ("n_blocks", i32)]
+                ("ghost", vp), ("n_blocks", i32)]
 
 
 class ParentView(C.Structure):
@@ -126,6 +126,7 @@ _SIGS = {
     "ol_surface_forces_scratch_doubles": (C.c_size_t, [i32]),
     "ol_flow_stats": (C.c_int, [vp, vp, vp, i32, vp, C.POINTER(C.c_double), vp]),
     "ol_flow_stats_scratch_doubles": (C.c_size_t, [i32]),
+    "ol_ghost_floats": (C.c_int64, [i32]),
     "ol_ctx_create": (C.c_int, [C.POINTER(vp), C.c_int, C.c_size_t, C.c_int]),
     "ol_ctx_destroy": (C.c_int, [vp]),
     "ol_ctx_case_footprint": (C.c_int, [vp, C.POINTER(CaseDesc), C.POINTER(C.c_size_t)]),
@@ -133,6 +134,7 @@ _SIGS = {
     "ol_ctx_case_remove": (C.c_int, [vp, i32]),
     "ol_ctx_step": (C.c_int, [vp, i32]),
     "ol_ctx_sync": (C.c_int, [vp]),
+    "ol_ctx_step_timed": (C.c_int, [vp, i32, C.POINTER(C.c_float)]),
     "ol_ctx_case_forces": (C.c_int, [vp, i32, C.POINTER(C.c_double)]),
     "ol_ctx_case_download": (C.c_int, [vp, i32, i32, vp, vp, vp]),
     "ol_ctx_case_info": (C.c_int, [vp, i32, C.POINTER(C.c_int64), C.POINTER(i32)]),

@@ -65,6 +65,7 @@ struct LevelDev {
   ol_step_params sp;
   int32_t *status;        // device watchdog word (may be null)
   const uint32_t *halo_tab;  // staging table (stream_collide.cuh)
+  float *ghost;           // absent-neighbour pull sources, kHaloEntries per block, or null
 };
 
 // One unit of batched work: block `block` of the level described by

@@ -121,14 +121,16 @@ __global__ void __launch_bounds__(512, OP == OL_OP_CUMULANT ? 2 : 1)
     copy_desc(&L, descs + w.desc, t);
     if (DDF) copy_desc(&D, tdescs + w.desc, t);
     __syncthreads();
-    load_nbbase(L.nbr, L.nbr_stride, L.block_offset, w.block, t, nbbase);
+    const bool miss = load_nbbase_sync(L.nbr, L.nbr_stride, L.block_offset, w.block, t, nbbase);
+    const size_t own = (size_t)nbbase[13] + t;
+    const bool obs = L.obstacle[own] != 0;
+    const float spg = L.sponge[own];
+    stage_flow<ST>(L, nbbase, w.block, t, E, miss);
     __syncthreads();
-    stage_flow<ST>(L, nbbase, w.block, t, E);
-    __syncthreads();
-    stream_collide_cell<OP, ST, WALE>(L, nbbase, E, w.block, t);
+    stream_collide_cell<OP, ST, WALE>(L, nbbase, E, w.block, t, obs, spg);
     if (DDF) {
       __syncthreads();
-      stage_thermal<ST>(D, nbbase, w.block, t, E, L.halo_tab);
+      stage_thermal<ST>(D, nbbase, w.block, t, E, L.halo_tab, miss);
       __syncthreads();
       thermal_cell<ST>(D, nbbase, E, w.block, t);
     }
@@ -281,7 +283,9 @@ struct ol_ctx {
   int64_t launches_per_step = 0;
   cudaGraphExec_t exec = nullptr;
   bool dirty = true;
-  int grid_mult = 1;  // persistent grid = grid_mult * resident CTAs, 0 = one CTA per item
+  // persistent grid = grid_mult * resident CTAs; 0 = one CTA per item;
+  // -1 = software-pipelined kernel (FP32 without DDF)
+  int grid_mult = 0;
   int64_t launches = 0;
   double *d_out = nullptr;
   std::mutex mu;
@@ -368,7 +372,7 @@ static int kernel_occupancy(int op) { return op == OL_OP_CUMULANT ? 2 : 1; }
 
 template <int OP, class ST, bool WALE, bool DDF>
 static void launch_variant(ol_ctx *c, const Launch &l) {
-  if (std::is_same<ST, StoreF32>::value && !DDF && c->grid_mult != 0) {
+  if (std::is_same<ST, StoreF32>::value && !DDF && c->grid_mult < 0) {
     // software-pipelined persistent kernel: one CTA per SM
     const int64_t grid = std::min<int64_t>(l.n, (int64_t)c->n_sm);
     k_sc_pipe<OP, WALE, true><<<(unsigned)grid, BCELLS, kPipeBytes, c->stream>>>(
@@ -849,6 +853,31 @@ extern "C" int ol_ctx_step(ol_ctx *c, int32_t n) {
   return OL_OK;
 }
 
+extern "C" int ol_ctx_step_timed(ol_ctx *c, int32_t n, float *ms) {
+  OL_CHECK_ARG(c && ms && n >= 0, "ol_ctx_step_timed: bad argument");
+  {
+    std::lock_guard<std::mutex> lk(c->mu);
+    OL_CUDA(cudaSetDevice(c->device));
+    if (c->dirty) {
+      const int rc = rebuild(c);
+      if (rc) return rc;
+    }
+  }
+  cudaEvent_t e0, e1;
+  OL_CUDA(cudaEventCreate(&e0));
+  OL_CUDA(cudaEventCreate(&e1));
+  OL_CUDA(cudaEventRecord(e0, c->stream));
+  int rc = ol_ctx_step(c, n);
+  if (rc == OL_OK) {
+    OL_CUDA(cudaEventRecord(e1, c->stream));
+    OL_CUDA(cudaEventSynchronize(e1));
+    OL_CUDA(cudaEventElapsedTime(ms, e0, e1));
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return rc;
+}
+
 extern "C" int ol_ctx_sync(ol_ctx *c) {
   OL_CHECK_ARG(c, "ol_ctx_sync: null context");
   OL_CUDA(cudaStreamSynchronize(c->stream));
@@ -952,7 +981,7 @@ extern "C" int ol_ctx_case_info(ol_ctx *c, int32_t id, int64_t *steps, int32_t *
 
 extern "C" int ol_ctx_autotune(ol_ctx *c, int32_t trials) {
   OL_CHECK_ARG(c && trials > 0, "ol_ctx_autotune: bad argument");
-  const int cands[4] = {1, 2, 4, 0};
+  const int cands[4] = {0, 1, 2, -1};
   float best_ms = 1e30f;
   int best = c->grid_mult;
   cudaEvent_t e0, e1;

@@ -27,28 +27,31 @@ __device__ __forceinline__ void cp_async_wait() {
 // Issue the asynchronous copies of block b's pull windows into E and fill
 // the slots of absent neighbours with their boundary values (FP32 storage).
 __device__ __forceinline__ void issue_stage_f32(const LevelDev &L, const int *nbbase, int b, int t,
-                                                float *E) {
+                                                float *E, bool any_missing) {
   const float *fin = (const float *)L.f_in;
   const int own = nbbase[13];
   const int eb = e_index(t & 7, (t >> 3) & 7, t >> 6);
   const float *src = fin + own + t;
+  const uint32_t *tab = L.halo_tab;
+  uint32_t te[kHaloPerThread];
+#pragma unroll
+  for (int j = 0; j < kHaloPerThread; ++j) {
+    const int i = t + j * BCELLS;
+    te[j] = i < kHaloEntries ? __ldg(tab + i) : 0xFFFFFFFFu;
+  }
 #pragma unroll
   for (int k = 0; k < 27; ++k) cp_async4(E + k * EPL + eb, src + (size_t)k * L.dstride);
-  const uint32_t *tab = L.halo_tab;
-#pragma unroll 1
-  for (int i = t; i < kHaloEntries; i += BCELLS) {
-    const uint32_t te = __ldg(tab + i);
-    const int k = te & 31, dir = (te >> 5) & 31, s = (te >> 10) & 511, dst = te >> 19;
+  const float *ghost_row = L.ghost ? L.ghost + (size_t)b * kHaloEntries : nullptr;
+#pragma unroll
+  for (int j = 0; j < kHaloPerThread; ++j) {
+    if (te[j] == 0xFFFFFFFFu) continue;
+    const int k = te[j] & 31, dir = (te[j] >> 5) & 31, s = (te[j] >> 10) & 511, dst = te[j] >> 19;
     const int nb = nbbase[dir];
-    if (nb >= 0) {
-      cp_async4(E + k * EPL + dst, fin + (size_t)k * L.dstride + nb + s);
-    } else {
-      const int sx = dst % 10 - 1, sy = (dst / 10) % 10 - 1, sz = dst / 100 - 1;
-      E[k * EPL + dst] =
-          pull_boundary<StoreF32>(L, k, b, sx + cx_of(k), sy + cy_of(k), sz + cz_of(k));
-    }
+    if (nb >= 0) cp_async4(E + k * EPL + dst, fin + (size_t)k * L.dstride + nb + s);
+    else if (ghost_row) cp_async4(E + k * EPL + dst, ghost_row + t + j * BCELLS);
   }
   cp_async_commit();
+  if (any_missing && !ghost_row) fill_missing_flow<StoreF32>(L, nbbase, b, t, E);
 }
 
 template <class DEV>
@@ -81,9 +84,8 @@ __global__ void __launch_bounds__(512, 1)
       __syncthreads();
     }
     const LevelDev &L = BATCHED ? Ls[buf] : L0;
-    load_nbbase(L.nbr, L.nbr_stride, L.block_offset, blk, t, nbb[buf]);
-    __syncthreads();
-    issue_stage_f32(L, nbb[buf], blk, t, smem + buf * 27 * EPL);
+    const bool miss = load_nbbase_sync(L.nbr, L.nbr_stride, L.block_offset, blk, t, nbb[buf]);
+    issue_stage_f32(L, nbb[buf], blk, t, smem + buf * 27 * EPL, miss);
     return blk;
   };
   int blk = prepare(0, it);
@@ -91,6 +93,10 @@ __global__ void __launch_bounds__(512, 1)
     const int cur = i & 1;
     const int nxt = it + gridDim.x;
     int nblk = -1;
+    const LevelDev &Lc = BATCHED ? Ls[cur] : L0;
+    const size_t own = (size_t)nbb[cur][13] + t;
+    const bool obs = Lc.obstacle[own] != 0;
+    const float spg = Lc.sponge[own];
     if (nxt < n) {
       nblk = prepare(cur ^ 1, nxt);
       cp_async_wait<1>();
@@ -98,8 +104,8 @@ __global__ void __launch_bounds__(512, 1)
       cp_async_wait<0>();
     }
     __syncthreads();
-    stream_collide_cell<OP, StoreF32, WALE>(BATCHED ? Ls[cur] : L0, nbb[cur],
-                                            smem + cur * 27 * EPL, blk, t);
+    stream_collide_cell<OP, StoreF32, WALE>(Lc, nbb[cur], smem + cur * 27 * EPL, blk, t, obs,
+                                            spg);
     __syncthreads();
     if (nxt >= n) break;
     it = nxt;

@@ -1,5 +1,6 @@
 // Drop-in stream-collide launch: one CTA per 8^3 block, one thread per cell,
 // caller buffers in the reference layout (FP32 populations).
+#include <cstdlib>
 #include <mutex>
 #include <vector>
 
@@ -26,6 +27,12 @@ static std::vector<uint32_t> build_halo_table() {
           const uint32_t dst = e_index(sx, sy, sz);
           tab.push_back((uint32_t)k | dir << 5 | src << 10 | dst << 19);
         }
+  // then the ring positions of the 10^3 staging plane, in slot order
+  for (int p = 0; p < 1000; ++p) {
+    const int x = p % 10 - 1, y = (p / 10) % 10 - 1, z = p / 100 - 1;
+    if (x >= 0 && x < 8 && y >= 0 && y < 8 && z >= 0 && z < 8) continue;
+    tab.push_back((uint32_t)p);
+  }
   return tab;
 }
 
@@ -37,7 +44,7 @@ const uint32_t *halo_table_device() {
   std::lock_guard<std::mutex> lk(mu);
   if (!per_dev[dev]) {
     const std::vector<uint32_t> tab = build_halo_table();
-    if ((int)tab.size() != kHaloEntries) return nullptr;
+    if ((int)tab.size() != kHaloEntries + kRingEntries) return nullptr;
     uint32_t *d = nullptr;
     if (cudaMalloc(&d, tab.size() * sizeof(uint32_t)) != cudaSuccess) return nullptr;
     if (cudaMemcpy(d, tab.data(), tab.size() * sizeof(uint32_t), cudaMemcpyHostToDevice) !=
@@ -60,11 +67,13 @@ __global__ void __launch_bounds__(512, OP == OL_OP_CUMULANT ? 2 : 1)
   __shared__ int nbbase[27];
   extern __shared__ float E[];
   const int b = blockIdx.x;
-  load_nbbase(L.nbr, L.nbr_stride, L.block_offset, b, threadIdx.x, nbbase);
+  const bool miss = load_nbbase_sync(L.nbr, L.nbr_stride, L.block_offset, b, threadIdx.x, nbbase);
+  const size_t own = (size_t)nbbase[13] + threadIdx.x;
+  const bool obs = L.obstacle[own] != 0;
+  const float spg = L.sponge[own];
+  stage_flow<ST>(L, nbbase, b, threadIdx.x, E, miss);
   __syncthreads();
-  stage_flow<ST>(L, nbbase, b, threadIdx.x, E);
-  __syncthreads();
-  stream_collide_cell<OP, ST, WALE>(L, nbbase, E, b, threadIdx.x);
+  stream_collide_cell<OP, ST, WALE>(L, nbbase, E, b, threadIdx.x, obs, spg);
 }
 
 template <int OP, class ST, bool WALE>
@@ -106,9 +115,26 @@ static void launch_sc(const LevelDev &L, cudaStream_t s) {
   }
 }
 
+// FP32 launches use one CTA per block (two resident per SM) with synchronous
+// staging; OL_PIPELINE=1 in the environment selects the software-pipelined
+// persistent kernel instead (one CTA per SM, cp.async double buffering).
+static bool use_pipeline() {
+  static int v = -1;
+  if (v < 0) {
+    const char *e = getenv("OL_PIPELINE");
+    v = (e && e[0] == '1') ? 1 : 0;
+  }
+  return v == 1;
+}
+
 void launch_stream_collide(const LevelDev &L, bool f16, cudaStream_t s) {
   if (L.n_blocks <= 0) return;
-  if (f16) {
+  if (L.ghost) {
+    if (f16) k_ghost_fill<StoreF16S><<<L.n_blocks, kGhostThreads, 0, s>>>(L);
+    else k_ghost_fill<StoreF32><<<L.n_blocks, kGhostThreads, 0, s>>>(L);
+  }
+  if (f16 || !use_pipeline()) {
+    if (!f16) { launch_sc<StoreF32>(L, s); return; }
     launch_sc<StoreF16S>(L, s);
   } else {
     const bool wale = L.sp.c_wale != 0.0f;
@@ -170,6 +196,7 @@ extern "C" int ol_stream_collide(const ol_level_view *lv, const ol_parent_view *
   L.dstride = (int64_t)BCELLS * lv->n_blocks;
   L.nbr_stride = lv->n_blocks;
   L.scale = 1.0f; L.inv_scale = 1.0f; L.p_inv_scale = 1.0f;
+  L.ghost = lv->ghost;
   L.sp = *sp;
   OL_CHECK_ARG((int64_t)lv->n_blocks * BCELLS < (1LL << 31),
                "ol_stream_collide: n_blocks too large for 32-bit plane offsets");
@@ -191,6 +218,10 @@ extern "C" int ol_stream_collide(const ol_level_view *lv, const ol_parent_view *
   launch_stream_collide(L, false, (cudaStream_t)stream);
   OL_LAUNCHED("ol_stream_collide");
   return OL_OK;
+}
+
+extern "C" int64_t ol_ghost_floats(int32_t n_blocks) {
+  return n_blocks > 0 ? (int64_t)n_blocks * kHaloEntries : 0;
 }
 
 extern "C" int ol_init_equilibrium(float *f, float *f_temp, float *f_old, float *rho_old,

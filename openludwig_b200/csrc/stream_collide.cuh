@@ -14,91 +14,131 @@
 namespace ol {
 
 // ---------------------------------------------------------------------------
-// Coarse-to-fine ghost value (physics_interpolation.jl:4-127).
+// Coarse-to-fine ghost values (physics_interpolation.jl:4-127), split into
+// what a ghost position shares across directions (the parent stencil and the
+// blended, interpolated rho and u) and the per-direction population.
 // gx, gy, gz: 1-based fine-level global source coordinates.
 // ---------------------------------------------------------------------------
-template <class ST>
-__device__ __noinline__ float interp_parent(const LevelDev &L, int k, int gx,
-                                            int gy, int gz) {
-  const ol_step_params &sp = L.sp;
-  const float w = w_of(k);
-  const float cx = (float)cx_of(k), cy = (float)cy_of(k), cz = (float)cz_of(k);
+struct ParentStencil {
+  int64_t ci[8];     // parent cell of each trilinear corner, -1 when absent
+  float wx, wy, wz;  // trilinear weights
+};
+
+__device__ __forceinline__ void parent_stencil(const LevelDev &L, int gx, int gy, int gz,
+                                               ParentStencil &P) {
   const float pxc = ((float)gx - 0.5f) * 0.5f;
   const float pyc = ((float)gy - 0.5f) * 0.5f;
   const float pzc = ((float)gz - 0.5f) * 0.5f;
   int px0 = (int)floorf(pxc), py0 = (int)floorf(pyc), pz0 = (int)floorf(pzc);
   const int px1 = px0 + 1, py1 = py0 + 1, pz1 = pz0 + 1;
-  const float wx = pxc - (float)px0, wy = pyc - (float)py0, wz = pzc - (float)pz0;
+  P.wx = pxc - (float)px0;
+  P.wy = pyc - (float)py0;
+  P.wz = pzc - (float)pz0;
   px0 = max(1, px0); py0 = max(1, py0); pz0 = max(1, pz0);
-
-  const bool temporal = sp.use_temporal_interp == 1 && sp.temporal_weight < 0.99f;
-  const float tw = sp.temporal_weight;
-  float v[8][5];
-  bool ok[8];
 #pragma unroll
   for (int s = 0; s < 8; ++s) {
     const int pgx = (s & 1) ? px1 : px0;
     const int pgy = (s & 2) ? py1 : py0;
     const int pgz = (s & 4) ? pz1 : pz0;
     const int pbx = (pgx - 1) / BS + 1, pby = (pgy - 1) / BS + 1, pbz = (pgz - 1) / BS + 1;
-    ok[s] = false;
-    v[s][0] = w; v[s][1] = 1.0f; v[s][2] = 0.0f; v[s][3] = 0.0f; v[s][4] = 0.0f;
+    P.ci[s] = -1;
     if (pbx >= 1 && pbx <= L.pdim_x && pby >= 1 && pby <= L.pdim_y && pbz >= 1 &&
         pbz <= L.pdim_z) {
       const int pb = L.pptr[(pbx - 1) + L.pdim_x * ((pby - 1) + L.pdim_y * (pbz - 1))];
-      if (pb > 0) {
-        const int cell = (pgx - 1) % BS + BS * ((pgy - 1) % BS) + BS * BS * ((pgz - 1) % BS);
-        const size_t ci = (size_t)(L.p_block_offset + pb - 1) * BCELLS + cell;
-        const float fn = ST::load((const typename ST::T *)L.pf, ci + (size_t)k * L.p_dstride,
-                                  k, L.p_inv_scale);
-        const float rn = L.prho[ci];
-        const float uxn = L.pvel[ci], uyn = L.pvel[ci + L.p_dstride],
-                    uzn = L.pvel[ci + 2 * L.p_dstride];
-        if (temporal) {
-          const float fo = ST::load((const typename ST::T *)L.pf_old,
-                                    ci + (size_t)k * L.p_dstride, k, L.p_inv_scale);
-          const float ro = L.prho_old[ci];
-          const float uxo = L.pvel_old[ci], uyo = L.pvel_old[ci + L.p_dstride],
-                      uzo = L.pvel_old[ci + 2 * L.p_dstride];
-          v[s][0] = fo * (1.0f - tw) + fn * tw;
-          v[s][1] = ro * (1.0f - tw) + rn * tw;
-          v[s][2] = uxo * (1.0f - tw) + uxn * tw;
-          v[s][3] = uyo * (1.0f - tw) + uyn * tw;
-          v[s][4] = uzo * (1.0f - tw) + uzn * tw;
-        } else {
-          v[s][0] = fn; v[s][1] = rn; v[s][2] = uxn; v[s][3] = uyn; v[s][4] = uzn;
-        }
-        ok[s] = true;
+      if (pb > 0)
+        P.ci[s] = (int64_t)(L.p_block_offset + pb - 1) * BCELLS + (pgx - 1) % BS +
+                  BS * ((pgy - 1) % BS) + BS * BS * ((pgz - 1) % BS);
+    }
+  }
+}
+
+__device__ __forceinline__ float trilerp(const float (&v)[8], float wx, float wy, float wz) {
+  const float c00 = v[0] * (1.0f - wx) + v[1] * wx;
+  const float c01 = v[4] * (1.0f - wx) + v[5] * wx;
+  const float c10 = v[2] * (1.0f - wx) + v[3] * wx;
+  const float c11 = v[6] * (1.0f - wx) + v[7] * wx;
+  const float c0 = c00 * (1.0f - wy) + c10 * wy;
+  const float c1 = c01 * (1.0f - wy) + c11 * wy;
+  return c0 * (1.0f - wz) + c1 * wz;
+}
+
+// Parent rho, ux, uy, uz at the ghost position: each corner blended between
+// the parent's old and new state, missing corners replaced by the (possibly
+// missing, then rho = 1, u = 0) first corner, then trilinear.
+__device__ __forceinline__ void interp_moments(const LevelDev &L, const ParentStencil &P,
+                                               float (&r)[4]) {
+  const ol_step_params &sp = L.sp;
+  const bool temporal = sp.use_temporal_interp == 1 && sp.temporal_weight < 0.99f;
+  const float tw = sp.temporal_weight;
+  float v[4][8];
+#pragma unroll
+  for (int s = 0; s < 8; ++s) {
+    v[0][s] = 1.0f; v[1][s] = 0.0f; v[2][s] = 0.0f; v[3][s] = 0.0f;
+    const int64_t c = P.ci[s];
+    if (c >= 0) {
+      const float rn = L.prho[c], uxn = L.pvel[c], uyn = L.pvel[c + L.p_dstride],
+                  uzn = L.pvel[c + 2 * L.p_dstride];
+      if (temporal) {
+        const float ro = L.prho_old[c], uxo = L.pvel_old[c], uyo = L.pvel_old[c + L.p_dstride],
+                    uzo = L.pvel_old[c + 2 * L.p_dstride];
+        v[0][s] = ro * (1.0f - tw) + rn * tw;
+        v[1][s] = uxo * (1.0f - tw) + uxn * tw;
+        v[2][s] = uyo * (1.0f - tw) + uyn * tw;
+        v[3][s] = uzo * (1.0f - tw) + uzn * tw;
+      } else {
+        v[0][s] = rn; v[1][s] = uxn; v[2][s] = uyn; v[3][s] = uzn;
       }
     }
   }
-  // Missing samples fall back to the (possibly missing) first corner.
 #pragma unroll
   for (int s = 1; s < 8; ++s)
-    if (!ok[s])
+    if (P.ci[s] < 0)
 #pragma unroll
-      for (int i = 0; i < 5; ++i) v[s][i] = v[0][i];
-  float r[5];
+      for (int i = 0; i < 4; ++i) v[i][s] = v[i][0];
 #pragma unroll
-  for (int i = 0; i < 5; ++i) {
-    const float c00 = v[0][i] * (1.0f - wx) + v[1][i] * wx;
-    const float c01 = v[4][i] * (1.0f - wx) + v[5][i] * wx;
-    const float c10 = v[2][i] * (1.0f - wx) + v[3][i] * wx;
-    const float c11 = v[6][i] * (1.0f - wx) + v[7][i] * wx;
-    const float c0 = c00 * (1.0f - wy) + c10 * wy;
-    const float c1 = c01 * (1.0f - wy) + c11 * wy;
-    r[i] = c0 * (1.0f - wz) + c1 * wz;
+  for (int i = 0; i < 4; ++i) r[i] = trilerp(v[i], P.wx, P.wy, P.wz);
+}
+
+// Ghost population k: interpolated f_k split into equilibrium (from the
+// interpolated moments r) and non-equilibrium part, the latter rescaled by
+// (tau_f - 1/2) / (tau_c - 1/2) clamped to [0.01, 100].
+template <class ST>
+__device__ __forceinline__ float interp_population(const LevelDev &L, int k,
+                                                   const ParentStencil &P, const float (&r)[4]) {
+  const ol_step_params &sp = L.sp;
+  const bool temporal = sp.use_temporal_interp == 1 && sp.temporal_weight < 0.99f;
+  const float tw = sp.temporal_weight;
+  const float w = w_of(k);
+  const typename ST::T *pf = (const typename ST::T *)L.pf;
+  const typename ST::T *pfo = (const typename ST::T *)L.pf_old;
+  float v[8];
+#pragma unroll
+  for (int s = 0; s < 8; ++s) {
+    v[s] = w;
+    const int64_t c = P.ci[s];
+    if (c >= 0) {
+      const size_t a = (size_t)c + (size_t)k * L.p_dstride;
+      const float fn = ST::load(pf, a, k, L.p_inv_scale);
+      v[s] = temporal ? ST::load(pfo, a, k, L.p_inv_scale) * (1.0f - tw) + fn * tw : fn;
+    }
   }
-  const float fe = feq_auto(r[1], r[2], r[3], r[4], w, cx, cy, cz, sp.compressible_corr);
-  const float fneq = r[0] - fe;
+#pragma unroll
+  for (int s = 1; s < 8; ++s)
+    if (P.ci[s] < 0) v[s] = v[0];
+  const float fi = trilerp(v, P.wx, P.wy, P.wz);
+  const float fe = feq_auto(r[0], r[1], r[2], r[3], w, (float)cx_of(k), (float)cy_of(k),
+                            (float)cz_of(k), sp.compressible_corr);
+  const float fneq = fi - fe;
   const float tc = sp.tau_parent - 0.5f, tf = sp.tau_molecular - 0.5f;
   const float sc = tc > 1e-6f ? fminf(fmaxf(tf / tc, 0.01f), 100.0f) : 1.0f;
   return fe + fneq * sc;
 }
 
 // ---------------------------------------------------------------------------
-// Source value of a pull whose neighbour block is absent
-// (kernel_cumulant.jl:117-159).  x, y, z are 0-based local coordinates.
+// Source value of a pull whose neighbour block is absent and whose source
+// lies outside the domain or on level 1 (kernel_cumulant.jl:117-159); the
+// fine-level interface case (:153-155) is interp_population, filled by
+// fill_missing_flow.  x, y, z are 0-based local coordinates.
 // ---------------------------------------------------------------------------
 template <class ST>
 __device__ __noinline__ float pull_boundary(const LevelDev &L, int k, int b,
@@ -132,7 +172,6 @@ __device__ __noinline__ float pull_boundary(const LevelDev &L, int k, int b,
     return ST::load((const typename ST::T *)L.f_in, ci + (size_t)km * L.dstride, km,
                     L.inv_scale);
   }
-  if (sp.is_level_1 == 0) return interp_parent<ST>(L, k, sgx, sgy, sgz);
   return w;
 }
 
@@ -408,13 +447,196 @@ __host__ __device__ constexpr int e_index(int x, int y, int z) {
   return (x + 1) + 10 * (y + 1) + 100 * (z + 1);
 }
 
-template <class ST, class BC>
+// Boundary values of the staging slots whose neighbour block is absent.  One
+// call per thread, made only by CTAs whose block has an absent neighbour, so
+// the call and its register save/restore stay off the bulk path.
+template <class BC>
+__device__ __noinline__ void fill_missing_slots(const int *nbbase, int t, float *E,
+                                                const uint32_t *__restrict__ tab, BC bc) {
+  for (int i = t; i < kHaloEntries; i += BCELLS) {
+    const uint32_t te = __ldg(tab + i);
+    const int k = te & 31, dir = (te >> 5) & 31, dst = te >> 19;
+    if (nbbase[dir] >= 0) continue;
+    const int sx = dst % 10 - 1, sy = (dst / 10) % 10 - 1, sz = dst / 100 - 1;
+    E[k * EPL + dst] = bc(k, sx + cx_of(k), sy + cy_of(k), sz + cz_of(k));
+  }
+}
+
+// Ring positions of the staging plane (the 488 slots of the 10^3 plane
+// outside the 8^3 block), listed in the staging table after its halo entries.
+constexpr int kRingEntries = 1000 - 512;
+
+// Staging planes whose slot p is never read, for a ring position p with
+// outward offsets (ox, oy, oz): a direction k with c_a = o_a on the first
+// axis a where o_a != 0 would pull slot p into a cell at -2 or 9 on that
+// axis, outside the block.  Four of these (i = 0..3) hold the interpolated
+// rho, ux, uy, uz of an interface position between the two fill phases.
+__device__ __forceinline__ int stash_plane(int ox, int oy, int oz, int i) {
+  const int u = (i & 1) + 1, v = (i >> 1) + 1;
+  if (ox != 0) return (ox + 1) + 3 * u + 9 * v;
+  if (oy != 0) return u + 3 * (oy + 1) + 9 * v;
+  return u + 3 * v + 9 * (oz + 1);
+}
+
+// Boundary values of the flow staging slots whose neighbour block is absent.
+// Domain boundaries (inlet, outlet, free-slip mirrors) and level-1 gaps are
+// evaluated per slot by pull_boundary.  A fine-level interface slot needs the
+// parent's rho and u interpolated at its source position, which every
+// direction pulling from that position shares: phase 1 computes them once
+// per ring position (one thread each) into stash slots, phase 2 spreads the
+// (direction, slot) entries over all threads and interpolates only f_k.
+template <class ST>
+__device__ __noinline__ void fill_missing_flow(const LevelDev &L, const int *nbbase, int b, int t,
+                                               float *E) {
+  const ol_step_params &sp = L.sp;
+  const uint32_t *__restrict__ tab = L.halo_tab;
+  const bool fine = sp.is_level_1 == 0;
+  const int gx0 = (L.map_x[b] - 1) * BS + 1, gy0 = (L.map_y[b] - 1) * BS + 1,
+            gz0 = (L.map_z[b] - 1) * BS + 1;
+  if (fine) {
+    if (t < kRingEntries) {
+      const int p = (int)__ldg(tab + kHaloEntries + t);
+      const int sx = p % 10 - 1, sy = (p / 10) % 10 - 1, sz = p / 100 - 1;
+      const int ox = sx < 0 ? -1 : (sx > 7 ? 1 : 0);
+      const int oy = sy < 0 ? -1 : (sy > 7 ? 1 : 0);
+      const int oz = sz < 0 ? -1 : (sz > 7 ? 1 : 0);
+      const int sgx = gx0 + sx, sgy = gy0 + sy, sgz = gz0 + sz;
+      if (nbbase[(ox + 1) + 3 * (oy + 1) + 9 * (oz + 1)] < 0 && sgx >= 1 &&
+          sgx <= sp.nx_global && sgy >= 1 && sgy <= sp.ny_global && sgz >= 1 &&
+          sgz <= sp.nz_global) {
+        ParentStencil P;
+        parent_stencil(L, sgx, sgy, sgz, P);
+        float r[4];
+        interp_moments(L, P, r);
+#pragma unroll
+        for (int i = 0; i < 4; ++i) E[stash_plane(ox, oy, oz, i) * EPL + p] = r[i];
+      }
+    }
+    __syncthreads();
+  }
+  for (int i = t; i < kHaloEntries; i += BCELLS) {
+    const uint32_t te = __ldg(tab + i);
+    const int k = te & 31, dir = (te >> 5) & 31, p = te >> 19;
+    if (nbbase[dir] >= 0) continue;
+    const int sx = p % 10 - 1, sy = (p / 10) % 10 - 1, sz = p / 100 - 1;
+    const int sgx = gx0 + sx, sgy = gy0 + sy, sgz = gz0 + sz;
+    float v;
+    if (fine && sgx >= 1 && sgx <= sp.nx_global && sgy >= 1 && sgy <= sp.ny_global &&
+        sgz >= 1 && sgz <= sp.nz_global) {
+      const int ox = sx < 0 ? -1 : (sx > 7 ? 1 : 0);
+      const int oy = sy < 0 ? -1 : (sy > 7 ? 1 : 0);
+      const int oz = sz < 0 ? -1 : (sz > 7 ? 1 : 0);
+      float r[4];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) r[j] = E[stash_plane(ox, oy, oz, j) * EPL + p];
+      ParentStencil P;
+      parent_stencil(L, sgx, sgy, sgz, P);
+      v = interp_population<ST>(L, k, P, r);
+    } else {
+      v = pull_boundary<ST>(L, k, b, sx + cx_of(k), sy + cy_of(k), sz + cz_of(k));
+    }
+    E[k * EPL + p] = v;
+  }
+}
+
+// Separate pass over the blocks of a level: the absent-neighbour pull sources
+// of block b, in staging-table order, into L.ghost[b * kHaloEntries + i].
+// Same values as fill_missing_flow; here the CTA is small, leaves the SM's
+// L1 to the parent gathers (a parent cell serves ~20 ghost slots), keeps the
+// whole parent stencil of each ring position in shared memory, and no
+// stream-collide CTA waits at a barrier while a few of its threads
+// interpolate.
+constexpr int kGhostThreads = 256;
+
+template <class ST>
+__global__ void __launch_bounds__(kGhostThreads)
+    k_ghost_fill(const __grid_constant__ LevelDev L) {
+  __shared__ int nbbase[27];
+  __shared__ float rs[4][kRingEntries];     // interpolated rho, ux, uy, uz
+  __shared__ int64_t cs[8][kRingEntries];   // parent stencil cells
+  __shared__ float ws[3][kRingEntries];     // trilinear weights
+  __shared__ int16_t ring_of[EPL];          // staging slot -> ring index
+  const int b = blockIdx.x, t = threadIdx.x;
+  int missing = 0;
+  if (t < 27) {
+    const int nb = L.nbr[b + L.nbr_stride * t];
+    nbbase[t] = nb > 0 ? (int)((L.block_offset + nb - 1) * BCELLS) : -1;
+    missing = nb <= 0;
+  }
+  if (!__syncthreads_or(missing)) return;
+  const ol_step_params &sp = L.sp;
+  const uint32_t *__restrict__ tab = L.halo_tab;
+  const bool fine = sp.is_level_1 == 0;
+  const int gx0 = (L.map_x[b] - 1) * BS + 1, gy0 = (L.map_y[b] - 1) * BS + 1,
+            gz0 = (L.map_z[b] - 1) * BS + 1;
+  if (fine) {
+    for (int q = t; q < kRingEntries; q += kGhostThreads) {
+      const int p = (int)__ldg(tab + kHaloEntries + q);
+      ring_of[p] = (int16_t)q;
+      const int sx = p % 10 - 1, sy = (p / 10) % 10 - 1, sz = p / 100 - 1;
+      const int ox = sx < 0 ? -1 : (sx > 7 ? 1 : 0);
+      const int oy = sy < 0 ? -1 : (sy > 7 ? 1 : 0);
+      const int oz = sz < 0 ? -1 : (sz > 7 ? 1 : 0);
+      const int sgx = gx0 + sx, sgy = gy0 + sy, sgz = gz0 + sz;
+      if (nbbase[(ox + 1) + 3 * (oy + 1) + 9 * (oz + 1)] < 0 && sgx >= 1 &&
+          sgx <= sp.nx_global && sgy >= 1 && sgy <= sp.ny_global && sgz >= 1 &&
+          sgz <= sp.nz_global) {
+        ParentStencil P;
+        parent_stencil(L, sgx, sgy, sgz, P);
+        float r[4];
+        interp_moments(L, P, r);
+#pragma unroll
+        for (int i = 0; i < 4; ++i) rs[i][q] = r[i];
+#pragma unroll
+        for (int s = 0; s < 8; ++s) cs[s][q] = P.ci[s];
+        ws[0][q] = P.wx; ws[1][q] = P.wy; ws[2][q] = P.wz;
+      }
+    }
+    __syncthreads();
+  }
+  float *G = L.ghost + (size_t)b * kHaloEntries;
+  for (int i = t; i < kHaloEntries; i += kGhostThreads) {
+    const uint32_t te = __ldg(tab + i);
+    const int k = te & 31, dir = (te >> 5) & 31, p = te >> 19;
+    if (nbbase[dir] >= 0) continue;
+    const int sx = p % 10 - 1, sy = (p / 10) % 10 - 1, sz = p / 100 - 1;
+    const int sgx = gx0 + sx, sgy = gy0 + sy, sgz = gz0 + sz;
+    float v;
+    if (fine && sgx >= 1 && sgx <= sp.nx_global && sgy >= 1 && sgy <= sp.ny_global &&
+        sgz >= 1 && sgz <= sp.nz_global) {
+      const int q = ring_of[p];
+      ParentStencil P;
+#pragma unroll
+      for (int s = 0; s < 8; ++s) P.ci[s] = cs[s][q];
+      P.wx = ws[0][q]; P.wy = ws[1][q]; P.wz = ws[2][q];
+      const float r[4] = {rs[0][q], rs[1][q], rs[2][q], rs[3][q]};
+      v = interp_population<ST>(L, k, P, r);
+    } else {
+      v = pull_boundary<ST>(L, k, b, sx + cx_of(k), sy + cy_of(k), sz + cz_of(k));
+    }
+    G[i] = v;
+  }
+}
+
+constexpr int kHaloPerThread = (kHaloEntries + BCELLS - 1) / BCELLS;  // 7
+
+// ghost_row: this block's precomputed absent-neighbour values in table order
+// (kHaloEntries floats), or null to compute them here with `fill`.
+template <class ST, class FILL>
 __device__ __forceinline__ void stage_block(const void *f_in_v, int64_t dstride, float inv_scale,
                                             const int *nbbase, int t, float *E,
-                                            const uint32_t *__restrict__ tab, BC bc) {
+                                            const uint32_t *__restrict__ tab, bool any_missing,
+                                            const float *__restrict__ ghost_row, FILL fill) {
   using T = typename ST::T;
   const T *__restrict__ fin = (const T *)f_in_v;
   const int own = nbbase[13];
+  // halo sources: all table entries and source values of this thread in flight at once
+  uint32_t te[kHaloPerThread];
+#pragma unroll
+  for (int j = 0; j < kHaloPerThread; ++j) {
+    const int i = t + j * BCELLS;
+    te[j] = i < kHaloEntries ? __ldg(tab + i) : 0xFFFFFFFFu;
+  }
   if (ST::kBytes == 4) {
     const int c0 = (t & 127) * 4;
     const int dst = e_index(c0 & 7, (c0 >> 3) & 7, c0 >> 6);
@@ -447,42 +669,58 @@ __device__ __forceinline__ void stage_block(const void *f_in_v, int64_t dstride,
       }
     }
   }
-#pragma unroll 1
-  for (int i = t; i < kHaloEntries; i += BCELLS) {
-    const uint32_t te = __ldg(tab + i);
-    const int k = te & 31, dir = (te >> 5) & 31, src = (te >> 10) & 511, dst = te >> 19;
-    const int nb = nbbase[dir];
-    float v;
-    if (nb >= 0) {
-      v = ST::load(fin, (size_t)k * dstride + nb + src, k, inv_scale);
-    } else {
-      const int sx = dst % 10 - 1, sy = (dst / 10) % 10 - 1, sz = dst / 100 - 1;
-      v = bc(k, sx + cx_of(k), sy + cy_of(k), sz + cz_of(k));
+  float hv[kHaloPerThread];
+  int hd[kHaloPerThread];
+#pragma unroll
+  for (int j = 0; j < kHaloPerThread; ++j) {
+    hd[j] = -1;
+    hv[j] = 0.0f;
+    if (te[j] != 0xFFFFFFFFu) {
+      const int k = te[j] & 31, dir = (te[j] >> 5) & 31, src = (te[j] >> 10) & 511;
+      const int nb = nbbase[dir];
+      if (nb >= 0) {
+        hd[j] = k * EPL + (int)(te[j] >> 19);
+        hv[j] = ST::load(fin, (size_t)k * dstride + nb + src, k, inv_scale);
+      } else if (ghost_row) {
+        hd[j] = k * EPL + (int)(te[j] >> 19);
+        hv[j] = ghost_row[t + j * BCELLS];
+      }
     }
-    E[k * EPL + dst] = v;
   }
+#pragma unroll
+  for (int j = 0; j < kHaloPerThread; ++j)
+    if (hd[j] >= 0) E[hd[j]] = hv[j];
+  if (any_missing && !ghost_row) fill();
 }
 
-// Neighbour-table row -> element offsets of the 27 neighbour blocks.
-__device__ __forceinline__ void load_nbbase(const int32_t *nbr, int64_t nbr_stride,
-                                            int64_t block_offset, int b, int t, int *nbbase) {
+// Neighbour-table row -> element offsets of the 27 neighbour blocks, then a
+// barrier; returns whether any neighbour of the block is absent.
+__device__ __forceinline__ bool load_nbbase_sync(const int32_t *nbr, int64_t nbr_stride,
+                                                 int64_t block_offset, int b, int t, int *nbbase) {
+  int missing = 0;
   if (t < 27) {
     const int nb = nbr[b + nbr_stride * t];
     nbbase[t] = nb > 0 ? (int)((block_offset + nb - 1) * BCELLS) : -1;
+    missing = nb <= 0;
   }
+  return __syncthreads_or(missing) != 0;
 }
 
 // Stage the flow populations of block b of level L.
 template <class ST>
 __device__ __forceinline__ void stage_flow(const LevelDev &L, const int *nbbase, int b, int t,
-                                           float *E) {
-  stage_block<ST>(L.f_in, L.dstride, L.inv_scale, nbbase, t, E, L.halo_tab,
-                  [&](int k, int x, int y, int z) { return pull_boundary<ST>(L, k, b, x, y, z); });
+                                           float *E, bool any_missing) {
+  const float *ghost_row = L.ghost ? L.ghost + (size_t)b * kHaloEntries : nullptr;
+  stage_block<ST>(L.f_in, L.dstride, L.inv_scale, nbbase, t, E, L.halo_tab, any_missing,
+                  ghost_row, [&]() { fill_missing_flow<ST>(L, nbbase, b, t, E); });
 }
 
+// obs / spg: this cell's obstacle flag and sponge weight, loaded by the
+// caller before staging so that their latency overlaps it.
 template <int OP, class ST, bool WALE>
 __device__ __forceinline__ void stream_collide_cell(const LevelDev &L, const int *nbbase,
-                                                    const float *E, int b, int t) {
+                                                    const float *E, int b, int t, bool obs,
+                                                    float spg) {
   using T = typename ST::T;
   const int x = t & 7, y = (t >> 3) & 7, z = t >> 6;
   const ol_step_params &sp = L.sp;
@@ -509,7 +747,7 @@ __device__ __forceinline__ void stream_collide_cell(const LevelDev &L, const int
   }
 
   float *fpost = (sp.store_post_collision && L.f_post) ? L.f_post : nullptr;
-  if (L.obstacle[own]) {
+  if (obs) {
     L.vel_out[own] = 0.0f;
     L.vel_out[own + L.dstride] = 0.0f;
     L.vel_out[own + 2 * L.dstride] = 0.0f;
@@ -524,7 +762,6 @@ __device__ __forceinline__ void stream_collide_cell(const LevelDev &L, const int
   rho = fmaxf(rho, 0.01f);
   const float inv_rho = 1.0f / rho;
   float ux = jx * inv_rho, uy = jy * inv_rho, uz = jz * inv_rho;
-  const float spg = L.sponge[own];
   if (spg > 0.0f) {
     rho = rho * (1.0f - spg) + 1.0f * spg;
     ux = ux * (1.0f - spg) + sp.u_inlet * spg;

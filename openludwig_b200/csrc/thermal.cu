@@ -9,9 +9,8 @@ __global__ void __launch_bounds__(512, 2) k_thermal(const __grid_constant__ Ther
   __shared__ int nbbase[27];
   extern __shared__ float E[];
   const int b = blockIdx.x;
-  load_nbbase(D.nbr, D.nbr_stride, D.block_offset, b, threadIdx.x, nbbase);
-  __syncthreads();
-  stage_thermal<ST>(D, nbbase, b, threadIdx.x, E, D.halo_tab);
+  const bool miss = load_nbbase_sync(D.nbr, D.nbr_stride, D.block_offset, b, threadIdx.x, nbbase);
+  stage_thermal<ST>(D, nbbase, b, threadIdx.x, E, D.halo_tab, miss);
   __syncthreads();
   thermal_cell<ST>(D, nbbase, E, b, threadIdx.x);
 }

@@ -131,11 +131,13 @@ __device__ __noinline__ float pull_boundary_thermal(const ThermalDev &D, int k, 
 // Stage the thermal populations of block b (same layout as the flow).
 template <class ST>
 __device__ __forceinline__ void stage_thermal(const ThermalDev &D, const int *nbbase, int b, int t,
-                                              float *E, const uint32_t *tab) {
-  stage_block<ST>(D.g_in, D.dstride, D.inv_scale, nbbase, t, E, tab,
-                  [&](int k, int x, int y, int z) {
-                    return pull_boundary_thermal<ST>(D, k, b, x, y, z);
-                  });
+                                              float *E, const uint32_t *tab, bool any_missing) {
+  const ThermalDev *Dp = &D;
+  stage_block<ST>(D.g_in, D.dstride, D.inv_scale, nbbase, t, E, tab, any_missing, nullptr, [&]() {
+    fill_missing_slots(nbbase, t, E, tab, [Dp, b](int k, int x, int y, int z) {
+      return pull_boundary_thermal<ST>(*Dp, k, b, x, y, z);
+    });
+  });
 }
 
 template <class ST>

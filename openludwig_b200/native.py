@@ -232,6 +232,12 @@ class Context:
     def step(self, n: int = 1) -> None:
         N.call("ol_ctx_step", self._h, n)
 
+    def step_timed(self, n: int) -> float:
+        """Advance n coarse steps; device milliseconds from CUDA events."""
+        ms = C.c_float()
+        N.call("ol_ctx_step_timed", self._h, n, C.byref(ms))
+        return float(ms.value)
+
     def sync(self) -> None:
         N.call("ol_ctx_sync", self._h)
 

@@ -67,6 +67,8 @@ class DeviceLevel:
     cell_z: torch.Tensor | None = None
     bouzidi_scratch: torch.Tensor | None = None
     f_post: torch.Tensor | None = None
+    # absent-neighbour pull sources, precomputed by a separate pass (optional)
+    ghost: torch.Tensor | None = None
     # thermal DDF
     g: torch.Tensor | None = None
     g_temp: torch.Tensor | None = None
@@ -91,8 +93,16 @@ class DeviceLevel:
 
 
 def upload_level(h: HostLevel, device: torch.device, ddf: bool = False, t_init: float = 1.0,
-                 reference_bouzidi: bool = False) -> DeviceLevel:
-    """adapt(backend, g) + the initial state of main.jl:113-173."""
+                 reference_bouzidi: bool = False, ghost: bool | None = None) -> DeviceLevel:
+    """adapt(backend, g) + the initial state of main.jl:113-173.
+
+    ghost: allocate the level's ol_level_view.ghost scratch, so that the
+    boundary values of absent neighbours are evaluated by their own pass
+    (identical results).  None = on refined levels only: their level
+    interfaces need coarse-to-fine interpolation, which that pass makes
+    cheaper; level 1 only has the cheap domain-boundary values."""
+    if ghost is None:
+        ghost = h.level_id > 1
     n = h.n_blocks
     S = 512 * n
     dev = device
@@ -120,6 +130,9 @@ def upload_level(h: HostLevel, device: torch.device, ddf: bool = False, t_init: 
         lv.bouzidi_scratch = torch.empty(27 * h.n_boundary, dtype=torch.float32, device=dev)
         if reference_bouzidi:
             lv.f_post = torch.zeros(S * 27, dtype=torch.float32, device=dev)
+    if ghost:
+        lv.ghost = torch.empty(int(N.lib().ol_ghost_floats(N.i32(n))), dtype=torch.float32,
+                               device=dev)
     if ddf:
         w = torch.tensor(lattice_weights(), dtype=torch.float32, device=dev)
         lv.g = (w[:, None] * t_init).expand(27, S).reshape(-1).clone()
@@ -235,7 +248,7 @@ def perform_timestep(s: StepSettings, lv: DeviceLevel, parent: ParentRef | None,
                        obstacle=_ptr(lv.obstacle), sponge=_ptr(lv.sponge),
                        wall_dist=_ptr(lv.wall_dist), neighbor_table=_ptr(lv.neighbor_table),
                        map_x=_ptr(lv.map_x), map_y=_ptr(lv.map_y), map_z=_ptr(lv.map_z),
-                       n_blocks=n)
+                       ghost=_ptr(lv.ghost), n_blocks=n)
     pv = N.ParentView()
     if parent is not None:
         p = parent.lv

@@ -80,7 +80,14 @@ def test_single_step_matches_oracle(case1, var):
                        map_x=S._ptr(arrs["map_x"]), map_y=S._ptr(arrs["map_y"]),
                        map_z=S._ptr(arrs["map_z"]), n_blocks=n)
     N.call("ol_stream_collide", C.byref(view), C.byref(N.ParentView()), C.byref(sp), S._stream())
+    # the same step with the boundary values of absent neighbours from their own pass
+    ghost = torch.empty(int(N.lib().ol_ghost_floats(N.i32(n))), dtype=torch.float32, device=DEV)
+    d_fout2, d_vout2 = torch.zeros_like(d_fout), torch.zeros_like(d_vout)
+    view2 = N.LevelView(**{name: getattr(view, name) for name, _ in N.LevelView._fields_})
+    view2.f_out, view2.vel_out, view2.ghost = S._ptr(d_fout2), S._ptr(d_vout2), S._ptr(ghost)
+    N.call("ol_stream_collide", C.byref(view2), C.byref(N.ParentView()), C.byref(sp), S._stream())
     torch.cuda.synchronize()
+    assert torch.equal(d_fout, d_fout2) and torch.equal(d_vout, d_vout2)
     # oracle
     o_fout = np.zeros(27 * 512 * n, np.float32)
     o_rho = np.zeros(512 * n, np.float32)
@@ -97,8 +104,8 @@ def test_single_step_matches_oracle(case1, var):
     assert max_abs(d_vout.cpu().numpy(), o_vout) < 2e-6
 
 
-def _run_gpu(hosts, p, st, steps, u, ddf=False):
-    levels = [S.upload_level(h, DEV, ddf=ddf) for h in hosts]
+def _run_gpu(hosts, p, st, steps, u, ddf=False, ghost=None):
+    levels = [S.upload_level(h, DEV, ddf=ddf, ghost=ghost) for h in hosts]
     dims = (p.nx_coarse, p.ny_coarse, p.nz_coarse)
     for t in range(1, steps + 1):
         S.recursive_step(levels, st, 0, t, None, 0.0, u, dims)
@@ -164,6 +171,19 @@ def test_two_level_recursion():
     for lg, lo in zip(g, o):
         assert rel_err(lg.f_temp.cpu().numpy(), lo.f_temp) < 1e-4
         assert rel_err(lg.rho.cpu().numpy(), lo.rho) < 1e-5
+
+
+def test_ghost_pass_equals_inline_fill():
+    """Interface and domain-boundary values from the separate pass (ghost
+    scratch) and from the in-staging fill give the same bits."""
+    c, mesh, p, hosts = small_sphere_case(resolution=16, levels=2, c_wale=np.float32(0.5))
+    st = S.StepSettings.from_config(c, False)
+    a = _run_gpu(hosts, p, st, 6, 0.05, ghost=True)
+    b = _run_gpu(hosts, p, st, 6, 0.05, ghost=False)
+    for la, lb in zip(a, b):
+        assert la.ghost is not None and lb.ghost is None
+        assert torch.equal(la.f_temp, lb.f_temp) and torch.equal(la.f, lb.f)
+        assert torch.equal(la.vel_temp, lb.vel_temp) and torch.equal(la.rho, lb.rho)
 
 
 def test_two_level_thermal_ddf():
