@@ -65,7 +65,8 @@ struct LevelDev {
   ol_step_params sp;
   int32_t *status;        // device watchdog word (may be null)
   const uint32_t *halo_tab;  // staging table (stream_collide.cuh)
-  float *ghost;           // absent-neighbour pull sources, kHaloEntries per block, or null
+  float *ghost;           // absent-neighbour pull sources, kHaloEntries per row, or null
+  const int32_t *gidx;    // block -> ghost row (-1: none); null = row b for block b
 };
 
 // One unit of batched work: block `block` of the level described by

@@ -107,6 +107,18 @@ __device__ __forceinline__ void copy_desc(DEV *dst, const DEV *src, int t) {
   for (int i = t; i < n4; i += blockDim.x) d[i] = s[i];
 }
 
+// Boundary values of absent neighbours for the ghost blocks of many cases:
+// one CTA per (descriptor, block) item.
+template <class ST>
+__global__ void __launch_bounds__(kGhostThreads)
+    k_ghost_fill_b(const LevelDev *__restrict__ descs, const WorkItem *__restrict__ items) {
+  __shared__ __align__(16) LevelDev L;
+  const WorkItem w = items[blockIdx.x];
+  copy_desc(&L, descs + w.desc, threadIdx.x);
+  __syncthreads();
+  ghost_fill_block<ST>(L, w.block, ghost_row_of(L, w.block));
+}
+
 template <int OP, class ST, bool WALE, bool DDF>
 __global__ void __launch_bounds__(512, OP == OL_OP_CUMULANT ? 2 : 1)
     k_sc_batched(const LevelDev *__restrict__ descs, const ThermalDev *__restrict__ tdescs,
@@ -225,7 +237,25 @@ struct DevLevel {
   int32_t *cb = nullptr;
   int8_t *cx = nullptr, *cy = nullptr, *cz = nullptr;
   float tau = 0.5f, tau_g = 0.5f, scale = 1.0f;
+  // refined levels: precomputed absent-neighbour values of the blocks that
+  // have an absent neighbour (compact rows), block -> row index
+  float *ghost = nullptr;
+  int32_t *gidx = nullptr;
+  std::vector<int32_t> ghost_blocks;  // host copy of the blocks with a row
 };
+
+// Blocks of a level with at least one absent neighbour (neighbour table
+// nB x 27 column-major, 0 = absent).
+static std::vector<int32_t> blocks_with_absent_neighbour(const ol_level_desc &S) {
+  std::vector<int32_t> out;
+  for (int b = 0; b < S.n_blocks; ++b)
+    for (int d = 0; d < 27; ++d)
+      if (S.neighbor_table[b + (size_t)S.n_blocks * d] <= 0) {
+        out.push_back(b);
+        break;
+      }
+  return out;
+}
 
 struct NCase {
   int32_t id = -1;
@@ -247,7 +277,7 @@ struct NCase {
 };
 
 struct Launch {
-  int kind;     // 0 = stream-collide, 1 = bouzidi gather, 2 = bouzidi scatter
+  int kind;     // 0 = stream-collide, 1 = bouzidi gather, 2 = bouzidi scatter, 3 = ghost fill
   int op = 0, wale = 0, ddf = 0;
   int64_t off = 0, n = 0;   // items (kind 0) or links (kind 1/2)
 };
@@ -306,6 +336,9 @@ static size_t case_meta_bytes(const ol_case_desc *cd) {
     const ol_level_desc &L = cd->levels[l];
     b += (size_t)L.n_blocks * (27 + 3) * 4 + (size_t)L.dim_x * L.dim_y * L.dim_z * 4;
     b += (size_t)L.n_boundary * (27 * 2 + 4 + 3);
+    if (l > 0)
+      b += blocks_with_absent_neighbour(L).size() * kHaloEntries * sizeof(float) +
+           (size_t)L.n_blocks * sizeof(int32_t);
   }
   b += (size_t)cd->n_triangles * 7 * 4 + force_partial_rows(cd->n_triangles) * 9 * 8 + 256;
   return b;
@@ -352,6 +385,7 @@ static void free_case_meta(NCase &c) {
   for (auto &L : c.levels) {
     cudaFree(L.nbr); cudaFree(L.mx); cudaFree(L.my); cudaFree(L.mz); cudaFree(L.bptr);
     cudaFree(L.q); cudaFree(L.cb); cudaFree(L.cx); cudaFree(L.cy); cudaFree(L.cz);
+    cudaFree(L.ghost); cudaFree(L.gidx);
   }
   cudaFree(c.mesh);
   cudaFree(c.partials);
@@ -373,8 +407,8 @@ static int kernel_occupancy(int op) { return op == OL_OP_CUMULANT ? 2 : 1; }
 template <int OP, class ST, bool WALE, bool DDF>
 static void launch_variant(ol_ctx *c, const Launch &l) {
   if (std::is_same<ST, StoreF32>::value && !DDF && c->grid_mult < 0) {
-    // software-pipelined persistent kernel: one CTA per SM
-    const int64_t grid = std::min<int64_t>(l.n, (int64_t)c->n_sm);
+    // software-pipelined persistent kernel: all resident CTAs
+    const int64_t grid = std::min<int64_t>(l.n, (int64_t)c->n_sm * kernel_occupancy(OP));
     k_sc_pipe<OP, WALE, true><<<(unsigned)grid, BCELLS, kPipeBytes, c->stream>>>(
         LevelDev{}, c->d_descs, c->d_items + l.off, (int)l.n);
     return;
@@ -406,6 +440,13 @@ static void record_step(ol_ctx *c) {
     if (l.kind == 0) {
       if (c->f16) launch_sc_dispatch<StoreF16S>(c, l);
       else launch_sc_dispatch<StoreF32>(c, l);
+    } else if (l.kind == 3) {
+      if (c->f16)
+        k_ghost_fill_b<StoreF16S><<<(unsigned)l.n, kGhostThreads, 0, c->stream>>>(
+            c->d_descs, c->d_items + l.off);
+      else
+        k_ghost_fill_b<StoreF32><<<(unsigned)l.n, kGhostThreads, 0, c->stream>>>(
+            c->d_descs, c->d_items + l.off);
     } else {
       const unsigned g = (unsigned)((l.n + 255) / 256);
       const BouzItem *items = c->d_bitems + l.off / 27;
@@ -455,6 +496,7 @@ static int rebuild(ol_ctx *c) {
     std::map<int, std::vector<int>> groups;  // variant -> descriptor ids
     int64_t scratch_off = 0;
     std::vector<int> bz_flow, bz_therm;
+    std::vector<WorkItem> ghost_items;
     for (auto &kv : c->cases) {
       NCase &cs = *kv.second;
       if ((int)cs.levels.size() < l) continue;
@@ -484,6 +526,9 @@ static int rebuild(ol_ctx *c) {
         L.p_block_offset = PV.block_offset;
         L.p_dstride = dstride;
         L.p_inv_scale = 1.0f / PV.scale;
+        L.ghost = V.ghost;
+        L.gidx = V.gidx;
+        for (int32_t b : V.ghost_blocks) ghost_items.push_back(WorkItem{d, b});
       } else {
         L.sp.tau_parent = 0.5f;
         L.p_inv_scale = 1.0f;
@@ -536,6 +581,15 @@ static int rebuild(ol_ctx *c) {
           bdescs.push_back(B);
         }
       }
+    }
+    if (!ghost_items.empty()) {  // boundary values of the refined levels first
+      Launch gl{};
+      gl.kind = 3;
+      gl.off = (int64_t)items.size();
+      items.insert(items.end(), ghost_items.begin(), ghost_items.end());
+      gl.n = (int64_t)ghost_items.size();
+      c->plan.push_back(gl);
+      ++per_step;
     }
     for (auto &g : groups) {
       Launch ln{};
@@ -755,6 +809,14 @@ extern "C" int ol_ctx_case_add(ol_ctx *c, const ol_case_desc *cd, int32_t *case_
     } else {
       std::vector<float> far(nc, 100.0f);
       OL_CUDA(cudaMemcpy(c->wd + c0, far.data(), nc * 4, cudaMemcpyHostToDevice));
+    }
+    if (l > 0) {
+      V.ghost_blocks = blocks_with_absent_neighbour(S);
+      std::vector<int32_t> gi((size_t)S.n_blocks, -1);
+      for (size_t r = 0; r < V.ghost_blocks.size(); ++r) gi[V.ghost_blocks[r]] = (int32_t)r;
+      if ((rc = upload(&V.gidx, gi.data(), gi.size()))) return rc;
+      if (!V.ghost_blocks.empty())
+        OL_CUDA(cudaMalloc(&V.ghost, V.ghost_blocks.size() * kHaloEntries * sizeof(float)));
     }
     V.n_boundary = S.n_boundary;
     if (S.n_boundary > 0) {

@@ -1,16 +1,18 @@
-// Software-pipelined stream-collide: one persistent 512-thread CTA per SM
-// walks its share of the blocks with two staging buffers.  While block i is
-// being collided out of buffer i&1, the asynchronous copies (cp.async) of
-// block i+1's 27 pull windows are in flight into the other buffer, and the
-// boundary values of block i+1's absent neighbours are computed.  One CTA
-// per SM leaves 128 registers per thread for the cell update (no spills)
-// and 2 x 105 KB of shared memory for the two buffers.
+// Software-pipelined stream-collide: persistent 512-thread CTAs (two per SM
+// for the cumulant operator) each walk a share of the blocks with ONE
+// staging buffer.  A cell's 27 pulls are read from the buffer into registers
+// first; once every thread has them the buffer is free, so the asynchronous
+// copies (cp.async) of the next block's pull windows -- and the boundary
+// values of its absent neighbours -- are issued before the current block's
+// collision and land while it computes.  The memory latency of block i+1
+// hides behind the arithmetic of block i without a second buffer, so two
+// CTAs (2 x 105 KB) still fit per SM.
 #pragma once
 #include "stream_collide.cuh"
 
 namespace ol {
 
-constexpr int kPipeBytes = 2 * kStageBytes;
+constexpr int kPipeBytes = kStageBytes;
 
 __device__ __forceinline__ void cp_async4(float *dst_smem, const float *src) {
   const unsigned d = (unsigned)__cvta_generic_to_shared(dst_smem);
@@ -24,34 +26,32 @@ __device__ __forceinline__ void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
 }
 
-// Issue the asynchronous copies of block b's pull windows into E and fill
-// the slots of absent neighbours with their boundary values (FP32 storage).
-__device__ __forceinline__ void issue_stage_f32(const LevelDev &L, const int *nbbase, int b, int t,
+// Issue the asynchronous copies of block b's pull windows into E (FP32
+// storage).  Returns whether the slots of absent neighbours still need their
+// boundary values (fill_missing_flow): the caller runs that fill where no
+// cell's pulls are live in registers, since it is a call.
+__device__ __forceinline__ bool issue_stage_f32(const LevelDev &L, const int *nbbase, int b, int t,
                                                 float *E, bool any_missing) {
   const float *fin = (const float *)L.f_in;
   const int own = nbbase[13];
   const int eb = e_index(t & 7, (t >> 3) & 7, t >> 6);
   const float *src = fin + own + t;
   const uint32_t *tab = L.halo_tab;
-  uint32_t te[kHaloPerThread];
-#pragma unroll
-  for (int j = 0; j < kHaloPerThread; ++j) {
-    const int i = t + j * BCELLS;
-    te[j] = i < kHaloEntries ? __ldg(tab + i) : 0xFFFFFFFFu;
-  }
 #pragma unroll
   for (int k = 0; k < 27; ++k) cp_async4(E + k * EPL + eb, src + (size_t)k * L.dstride);
-  const float *ghost_row = L.ghost ? L.ghost + (size_t)b * kHaloEntries : nullptr;
-#pragma unroll
-  for (int j = 0; j < kHaloPerThread; ++j) {
-    if (te[j] == 0xFFFFFFFFu) continue;
-    const int k = te[j] & 31, dir = (te[j] >> 5) & 31, s = (te[j] >> 10) & 511, dst = te[j] >> 19;
+  const float *ghost_row = ghost_row_of(L, b);
+  // one table entry at a time: this runs while a cell's pulls are held in
+  // registers, so it keeps its own register footprint small
+#pragma unroll 1
+  for (int i = t; i < kHaloEntries; i += BCELLS) {
+    const uint32_t te = __ldg(tab + i);
+    const int k = te & 31, dir = (te >> 5) & 31, s = (te >> 10) & 511, dst = te >> 19;
     const int nb = nbbase[dir];
     if (nb >= 0) cp_async4(E + k * EPL + dst, fin + (size_t)k * L.dstride + nb + s);
-    else if (ghost_row) cp_async4(E + k * EPL + dst, ghost_row + t + j * BCELLS);
+    else if (ghost_row) cp_async4(E + k * EPL + dst, ghost_row + i);
   }
   cp_async_commit();
-  if (any_missing && !ghost_row) fill_missing_flow<StoreF32>(L, nbbase, b, t, E);
+  return any_missing && !ghost_row;
 }
 
 template <class DEV>
@@ -64,52 +64,59 @@ __device__ __forceinline__ void copy_words(DEV *dst, const DEV *src, int t) {
 
 // BATCHED = false: the blocks 0..n_blocks-1 of the level L0 (drop-in).
 // BATCHED = true : work items (descriptor, block) from `items`.
+// The per-item descriptor and neighbour offsets rotate through three slots:
+// the slot fetched in iteration i was last read by the collision of
+// iteration i-2, which every thread finished before iteration i-1's barriers.
 template <int OP, bool WALE, bool BATCHED>
-__global__ void __launch_bounds__(512, 1)
+__global__ void __launch_bounds__(512, OP == OL_OP_CUMULANT ? 2 : 1)
     k_sc_pipe(const __grid_constant__ LevelDev L0, const LevelDev *__restrict__ descs,
               const WorkItem *__restrict__ items, int n_items) {
-  extern __shared__ float smem[];
-  __shared__ __align__(16) LevelDev Ls[BATCHED ? 2 : 1];
-  __shared__ int nbb[2][27];
+  extern __shared__ float E[];
+  __shared__ __align__(16) LevelDev Ls[BATCHED ? 3 : 1];
+  __shared__ int nbb[3][27];
   const int t = threadIdx.x;
   const int n = BATCHED ? n_items : L0.n_blocks;
   int it = blockIdx.x;
   if (it >= n) return;
-  auto prepare = [&](int buf, int item) -> int {
-    int blk = item;
+  // descriptor + neighbour offsets of `item` into slot s (ends with a barrier)
+  auto fetch = [&](int s, int item, int &blk) -> bool {
+    blk = item;
     if (BATCHED) {
       const WorkItem w = items[item];
-      copy_words(&Ls[buf], descs + w.desc, t);
+      copy_words(&Ls[s], descs + w.desc, t);
       blk = w.block;
       __syncthreads();
     }
-    const LevelDev &L = BATCHED ? Ls[buf] : L0;
-    const bool miss = load_nbbase_sync(L.nbr, L.nbr_stride, L.block_offset, blk, t, nbb[buf]);
-    issue_stage_f32(L, nbb[buf], blk, t, smem + buf * 27 * EPL, miss);
-    return blk;
+    const LevelDev &L = BATCHED ? Ls[s] : L0;
+    return load_nbbase_sync(L.nbr, L.nbr_stride, L.block_offset, blk, t, nbb[s]);
   };
-  int blk = prepare(0, it);
-  for (int i = 0;; ++i) {
-    const int cur = i & 1;
-    const int nxt = it + gridDim.x;
-    int nblk = -1;
+  int cur = 0, blk = 0;
+  const bool miss0 = fetch(0, it, blk);
+  if (issue_stage_f32(BATCHED ? Ls[0] : L0, nbb[0], blk, t, E, miss0))
+    fill_missing_flow<StoreF32>(BATCHED ? Ls[0] : L0, nbb[0], blk, t, E);
+  for (;;) {
     const LevelDev &Lc = BATCHED ? Ls[cur] : L0;
     const size_t own = (size_t)nbb[cur][13] + t;
     const bool obs = Lc.obstacle[own] != 0;
     const float spg = Lc.sponge[own];
-    if (nxt < n) {
-      nblk = prepare(cur ^ 1, nxt);
-      cp_async_wait<1>();
-    } else {
-      cp_async_wait<0>();
-    }
-    __syncthreads();
-    stream_collide_cell<OP, StoreF32, WALE>(Lc, nbb[cur], smem + cur * 27 * EPL, blk, t, obs,
-                                            spg);
-    __syncthreads();
+    const int nxt = it + gridDim.x;
+    const int sn = cur == 2 ? 0 : cur + 1;
+    int nblk = -1;
+    bool nmiss = false;
+    if (nxt < n) nmiss = fetch(sn, nxt, nblk);
+    cp_async_wait<0>();
+    __syncthreads();  // block blk staged
+    float A[27];
+    load_pulls(E, t, A);
+    __syncthreads();  // staging buffer free
+    bool fill = false;
+    if (nxt < n) fill = issue_stage_f32(BATCHED ? Ls[sn] : L0, nbb[sn], nblk, t, E, nmiss);
+    collide_cell<OP, StoreF32, WALE>(Lc, nbb[cur], A, blk, t, obs, spg);
     if (nxt >= n) break;
+    if (fill) fill_missing_flow<StoreF32>(BATCHED ? Ls[sn] : L0, nbb[sn], nblk, t, E);
     it = nxt;
     blk = nblk;
+    cur = sn;
   }
 }
 

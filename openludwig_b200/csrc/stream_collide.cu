@@ -99,7 +99,8 @@ static void launch_pipe(const LevelDev &L, cudaStream_t s) {
     cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
     done = true;
   }
-  const int grid = L.n_blocks < n_sm ? L.n_blocks : n_sm;
+  const int resident = n_sm * (OP == OL_OP_CUMULANT ? 2 : 1);
+  const int grid = L.n_blocks < resident ? L.n_blocks : resident;
   k_sc_pipe<OP, WALE, false><<<grid, BCELLS, kPipeBytes, s>>>(L, nullptr, nullptr, 0);
 }
 
@@ -208,6 +209,8 @@ extern "C" int ol_stream_collide(const ol_level_view *lv, const ol_parent_view *
     OL_CHECK_ARG(!(sp->use_temporal_interp == 1 && sp->temporal_weight < 0.99f) ||
                      (pv->f_old && pv->rho_old && pv->vel_old),
                  "ol_stream_collide: temporal interpolation needs parent old state");
+    OL_CHECK_ARG((int64_t)pv->n_blocks * BCELLS < (1LL << 31),
+                 "ol_stream_collide: parent n_blocks too large for 32-bit cell indices");
     L.pf = pv->f; L.prho = pv->rho; L.pvel = pv->vel;
     L.pf_old = pv->f_old; L.prho_old = pv->rho_old; L.pvel_old = pv->vel_old;
     L.pptr = pv->block_ptr;

@@ -543,67 +543,117 @@ __device__ __noinline__ void fill_missing_flow(const LevelDev &L, const int *nbb
 // of block b, in staging-table order, into L.ghost[b * kHaloEntries + i].
 // Same values as fill_missing_flow; here the CTA is small, leaves the SM's
 // L1 to the parent gathers (a parent cell serves ~20 ghost slots), keeps the
-// whole parent stencil of each ring position in shared memory, and no
+// whole parent stencil of each ring position in shared memory, and spreads
+// only the slots that need a value over its threads (compacted lists), so no
 // stream-collide CTA waits at a barrier while a few of its threads
-// interpolate.
+// interpolate.  Parent cell indices are kept as int32 (the launch checks
+// that the parent's cells fit).
 constexpr int kGhostThreads = 256;
+constexpr int kGhostScan = (kHaloEntries + kGhostThreads - 1) / kGhostThreads;  // 13
 
+// Warp-aggregated append of `value` to a shared list when `flag` is set;
+// every lane of the warp makes the call.
+__device__ __forceinline__ void append_if(bool flag, int value, int *count, int16_t *list) {
+  const unsigned m = __ballot_sync(0xffffffffu, flag);
+  if (m == 0) return;
+  const int lane = threadIdx.x & 31, leader = __ffs(m) - 1;
+  int base = 0;
+  if (lane == leader) base = atomicAdd(count, __popc(m));
+  base = __shfl_sync(0xffffffffu, base, leader);
+  if (flag) list[base + __popc(m & ((1u << lane) - 1u))] = (int16_t)value;
+}
+
+// Row of block b in the ghost scratch of level L (null when the block has
+// no row: no scratch, or no absent neighbour under a compact index).
+__device__ __forceinline__ float *ghost_row_of(const LevelDev &L, int b) {
+  if (!L.ghost) return nullptr;
+  const int r = L.gidx ? L.gidx[b] : b;
+  return r >= 0 ? L.ghost + (size_t)r * kHaloEntries : nullptr;
+}
+
+// One CTA of kGhostThreads threads evaluates block b's row G.
 template <class ST>
-__global__ void __launch_bounds__(kGhostThreads)
-    k_ghost_fill(const __grid_constant__ LevelDev L) {
+__device__ __forceinline__ void ghost_fill_block(const LevelDev &L, int b, float *G) {
   __shared__ int nbbase[27];
+  __shared__ int n_pos, n_slot;
   __shared__ float rs[4][kRingEntries];     // interpolated rho, ux, uy, uz
-  __shared__ int64_t cs[8][kRingEntries];   // parent stencil cells
+  __shared__ int32_t cs[8][kRingEntries];   // parent stencil cells
   __shared__ float ws[3][kRingEntries];     // trilinear weights
   __shared__ int16_t ring_of[EPL];          // staging slot -> ring index
-  const int b = blockIdx.x, t = threadIdx.x;
+  __shared__ int16_t pos_list[kRingEntries];
+  __shared__ int16_t slot_list[kHaloEntries];
+  const int t = threadIdx.x;
   int missing = 0;
   if (t < 27) {
     const int nb = L.nbr[b + L.nbr_stride * t];
     nbbase[t] = nb > 0 ? (int)((L.block_offset + nb - 1) * BCELLS) : -1;
     missing = nb <= 0;
   }
+  if (t == 0) { n_pos = 0; n_slot = 0; }
   if (!__syncthreads_or(missing)) return;
   const ol_step_params &sp = L.sp;
   const uint32_t *__restrict__ tab = L.halo_tab;
   const bool fine = sp.is_level_1 == 0;
   const int gx0 = (L.map_x[b] - 1) * BS + 1, gy0 = (L.map_y[b] - 1) * BS + 1,
             gz0 = (L.map_z[b] - 1) * BS + 1;
+  auto in_domain = [&](int gx, int gy, int gz) {
+    return gx >= 1 && gx <= sp.nx_global && gy >= 1 && gy <= sp.ny_global && gz >= 1 &&
+           gz <= sp.nz_global;
+  };
+  // lists: interface ring positions and slots whose neighbour is absent
+  uint32_t te[kGhostScan];
+#pragma unroll
+  for (int j = 0; j < kGhostScan; ++j) {
+    const int i = t + j * kGhostThreads;
+    te[j] = i < kHaloEntries ? __ldg(tab + i) : 0u;
+  }
   if (fine) {
-    for (int q = t; q < kRingEntries; q += kGhostThreads) {
-      const int p = (int)__ldg(tab + kHaloEntries + q);
-      ring_of[p] = (int16_t)q;
-      const int sx = p % 10 - 1, sy = (p / 10) % 10 - 1, sz = p / 100 - 1;
-      const int ox = sx < 0 ? -1 : (sx > 7 ? 1 : 0);
-      const int oy = sy < 0 ? -1 : (sy > 7 ? 1 : 0);
-      const int oz = sz < 0 ? -1 : (sz > 7 ? 1 : 0);
-      const int sgx = gx0 + sx, sgy = gy0 + sy, sgz = gz0 + sz;
-      if (nbbase[(ox + 1) + 3 * (oy + 1) + 9 * (oz + 1)] < 0 && sgx >= 1 &&
-          sgx <= sp.nx_global && sgy >= 1 && sgy <= sp.ny_global && sgz >= 1 &&
-          sgz <= sp.nz_global) {
-        ParentStencil P;
-        parent_stencil(L, sgx, sgy, sgz, P);
-        float r[4];
-        interp_moments(L, P, r);
-#pragma unroll
-        for (int i = 0; i < 4; ++i) rs[i][q] = r[i];
-#pragma unroll
-        for (int s = 0; s < 8; ++s) cs[s][q] = P.ci[s];
-        ws[0][q] = P.wx; ws[1][q] = P.wy; ws[2][q] = P.wz;
+    for (int j = 0; j < (kRingEntries + kGhostThreads - 1) / kGhostThreads; ++j) {
+      const int q = t + j * kGhostThreads;
+      bool want = false;
+      if (q < kRingEntries) {
+        const int p = (int)__ldg(tab + kHaloEntries + q);
+        ring_of[p] = (int16_t)q;
+        const int sx = p % 10 - 1, sy = (p / 10) % 10 - 1, sz = p / 100 - 1;
+        const int ox = sx < 0 ? -1 : (sx > 7 ? 1 : 0);
+        const int oy = sy < 0 ? -1 : (sy > 7 ? 1 : 0);
+        const int oz = sz < 0 ? -1 : (sz > 7 ? 1 : 0);
+        want = nbbase[(ox + 1) + 3 * (oy + 1) + 9 * (oz + 1)] < 0 &&
+               in_domain(gx0 + sx, gy0 + sy, gz0 + sz);
       }
+      append_if(want, q, &n_pos, pos_list);
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < kGhostScan; ++j) {
+    const int i = t + j * kGhostThreads;
+    append_if(i < kHaloEntries && nbbase[(te[j] >> 5) & 31] < 0, i, &n_slot, slot_list);
+  }
+  __syncthreads();
+  if (fine) {
+    for (int j = t; j < n_pos; j += kGhostThreads) {
+      const int q = pos_list[j];
+      const int p = (int)__ldg(tab + kHaloEntries + q);
+      const int sx = p % 10 - 1, sy = (p / 10) % 10 - 1, sz = p / 100 - 1;
+      ParentStencil P;
+      parent_stencil(L, gx0 + sx, gy0 + sy, gz0 + sz, P);
+      float r[4];
+      interp_moments(L, P, r);
+#pragma unroll
+      for (int i = 0; i < 4; ++i) rs[i][q] = r[i];
+#pragma unroll
+      for (int s = 0; s < 8; ++s) cs[s][q] = (int32_t)P.ci[s];
+      ws[0][q] = P.wx; ws[1][q] = P.wy; ws[2][q] = P.wz;
     }
     __syncthreads();
   }
-  float *G = L.ghost + (size_t)b * kHaloEntries;
-  for (int i = t; i < kHaloEntries; i += kGhostThreads) {
-    const uint32_t te = __ldg(tab + i);
-    const int k = te & 31, dir = (te >> 5) & 31, p = te >> 19;
-    if (nbbase[dir] >= 0) continue;
+  for (int j = t; j < n_slot; j += kGhostThreads) {
+    const int i = slot_list[j];
+    const uint32_t e = __ldg(tab + i);
+    const int k = e & 31, p = e >> 19;
     const int sx = p % 10 - 1, sy = (p / 10) % 10 - 1, sz = p / 100 - 1;
-    const int sgx = gx0 + sx, sgy = gy0 + sy, sgz = gz0 + sz;
     float v;
-    if (fine && sgx >= 1 && sgx <= sp.nx_global && sgy >= 1 && sgy <= sp.ny_global &&
-        sgz >= 1 && sgz <= sp.nz_global) {
+    if (fine && in_domain(gx0 + sx, gy0 + sy, gz0 + sz)) {
       const int q = ring_of[p];
       ParentStencil P;
 #pragma unroll
@@ -616,6 +666,13 @@ __global__ void __launch_bounds__(kGhostThreads)
     }
     G[i] = v;
   }
+}
+
+// Drop-in: one CTA per block of the level (rows indexed by block).
+template <class ST>
+__global__ void __launch_bounds__(kGhostThreads)
+    k_ghost_fill(const __grid_constant__ LevelDev L) {
+  ghost_fill_block<ST>(L, blockIdx.x, L.ghost + (size_t)blockIdx.x * kHaloEntries);
 }
 
 constexpr int kHaloPerThread = (kHaloEntries + BCELLS - 1) / BCELLS;  // 7
@@ -710,28 +767,45 @@ __device__ __forceinline__ bool load_nbbase_sync(const int32_t *nbr, int64_t nbr
 template <class ST>
 __device__ __forceinline__ void stage_flow(const LevelDev &L, const int *nbbase, int b, int t,
                                            float *E, bool any_missing) {
-  const float *ghost_row = L.ghost ? L.ghost + (size_t)b * kHaloEntries : nullptr;
+  const float *ghost_row = ghost_row_of(L, b);
   stage_block<ST>(L.f_in, L.dstride, L.inv_scale, nbbase, t, E, L.halo_tab, any_missing,
                   ghost_row, [&]() { fill_missing_flow<ST>(L, nbbase, b, t, E); });
 }
 
 // obs / spg: this cell's obstacle flag and sponge weight, loaded by the
 // caller before staging so that their latency overlaps it.
+// The 27 pulls of cell t from the staged windows.
+__device__ __forceinline__ void load_pulls(const float *E, int t, float (&A)[27]) {
+  const int eb = e_index(t & 7, (t >> 3) & 7, t >> 6);
+#pragma unroll
+  for (int k = 0; k < 27; ++k)
+    A[k] = E[k * EPL + eb - (cx_of(k) + 10 * cy_of(k) + 100 * cz_of(k))];
+}
+
+template <int OP, class ST, bool WALE>
+__device__ __forceinline__ void collide_cell(const LevelDev &L, const int *nbbase, float (&A)[27],
+                                             int b, int t, bool obs, float spg);
+
 template <int OP, class ST, bool WALE>
 __device__ __forceinline__ void stream_collide_cell(const LevelDev &L, const int *nbbase,
                                                     const float *E, int b, int t, bool obs,
                                                     float spg) {
+  float A[27];
+  load_pulls(E, t, A);
+  collide_cell<OP, ST, WALE>(L, nbbase, A, b, t, obs, spg);
+}
+
+// Everything after the pull: bounce-back, moments, sponge, wall model,
+// WALE, collision, forcing and the stores of cell t of block b.
+template <int OP, class ST, bool WALE>
+__device__ __forceinline__ void collide_cell(const LevelDev &L, const int *nbbase, float (&A)[27],
+                                             int b, int t, bool obs, float spg) {
   using T = typename ST::T;
   const int x = t & 7, y = (t >> 3) & 7, z = t >> 6;
   const ol_step_params &sp = L.sp;
   const size_t own = (size_t)nbbase[13] + t;
   T *__restrict__ fout = (T *)L.f_out;
 
-  float A[27];
-  const int eb = e_index(x, y, z);
-#pragma unroll
-  for (int k = 0; k < 27; ++k)
-    A[k] = E[k * EPL + eb - (cx_of(k) + 10 * cy_of(k) + 100 * cz_of(k))];
   float rho = 0.0f, jx = 0.0f, jy = 0.0f, jz = 0.0f;
 #pragma unroll
   for (int k = 0; k < 27; ++k) {
