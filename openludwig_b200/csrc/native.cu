@@ -133,11 +133,13 @@ __global__ void __launch_bounds__(512, OP == OL_OP_CUMULANT ? 2 : 1)
     copy_desc(&L, descs + w.desc, t);
     if (DDF) copy_desc(&D, tdescs + w.desc, t);
     __syncthreads();
+    const int64_t own0 = (L.block_offset + w.block) * BCELLS;
+    OwnRegs<ST> r;
+    own_load(L.f_in, L.dstride, own0, t, r);
+    const bool obs = L.obstacle[own0 + t] != 0;
+    const float spg = L.sponge[own0 + t];
     const bool miss = load_nbbase_sync(L.nbr, L.nbr_stride, L.block_offset, w.block, t, nbbase);
-    const size_t own = (size_t)nbbase[13] + t;
-    const bool obs = L.obstacle[own] != 0;
-    const float spg = L.sponge[own];
-    stage_flow<ST>(L, nbbase, w.block, t, E, miss);
+    stage_flow<ST>(L, nbbase, w.block, t, E, miss, r);
     __syncthreads();
     stream_collide_cell<OP, ST, WALE>(L, nbbase, E, w.block, t, obs, spg);
     if (DDF) {

@@ -67,11 +67,15 @@ __global__ void __launch_bounds__(512, OP == OL_OP_CUMULANT ? 2 : 1)
   __shared__ int nbbase[27];
   extern __shared__ float E[];
   const int b = blockIdx.x;
+  // the own block's planes and masks do not depend on the neighbour table:
+  // their loads are in flight while it is read
+  const int64_t own0 = (L.block_offset + b) * BCELLS;
+  OwnRegs<ST> r;
+  own_load(L.f_in, L.dstride, own0, threadIdx.x, r);
+  const bool obs = L.obstacle[own0 + threadIdx.x] != 0;
+  const float spg = L.sponge[own0 + threadIdx.x];
   const bool miss = load_nbbase_sync(L.nbr, L.nbr_stride, L.block_offset, b, threadIdx.x, nbbase);
-  const size_t own = (size_t)nbbase[13] + threadIdx.x;
-  const bool obs = L.obstacle[own] != 0;
-  const float spg = L.sponge[own];
-  stage_flow<ST>(L, nbbase, b, threadIdx.x, E, miss);
+  stage_flow<ST>(L, nbbase, b, threadIdx.x, E, miss, r);
   __syncthreads();
   stream_collide_cell<OP, ST, WALE>(L, nbbase, E, b, threadIdx.x, obs, spg);
 }

@@ -677,54 +677,84 @@ __global__ void __launch_bounds__(kGhostThreads)
 
 constexpr int kHaloPerThread = (kHaloEntries + BCELLS - 1) / BCELLS;  // 7
 
+// The own block's 27 planes, loaded into registers with 16-byte loads
+// (FP32: 7 float4 per thread; FP16: 4 x 8 halves).  The loads depend only on
+// the block's own offset, so a kernel can issue them before it has read the
+// neighbour table.
+template <class ST> struct OwnRegs;
+template <> struct OwnRegs<StoreF32> { float4 v[7]; };
+template <> struct OwnRegs<StoreF16S> { uint4 v[4]; };
+
+__device__ __forceinline__ void own_load(const void *f_in_v, int64_t dstride, int64_t own, int t,
+                                         OwnRegs<StoreF32> &r) {
+  const float *fin = (const float *)f_in_v;
+  const int c0 = (t & 127) * 4;
+#pragma unroll
+  for (int j = 0; j < 7; ++j) {
+    const int k = (t >> 7) + 4 * j;
+    if (k < 27) r.v[j] = __ldg((const float4 *)(fin + (size_t)k * dstride + own + c0));
+  }
+}
+__device__ __forceinline__ void own_load(const void *f_in_v, int64_t dstride, int64_t own, int t,
+                                         OwnRegs<StoreF16S> &r) {
+  const __half *fin = (const __half *)f_in_v;
+  const int c0 = (t & 63) * 8;
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const int k = (t >> 6) + 8 * j;
+    if (k < 27) r.v[j] = __ldg((const uint4 *)(fin + (size_t)k * dstride + own + c0));
+  }
+}
+__device__ __forceinline__ void own_store(const OwnRegs<StoreF32> &r, float, int t, float *E) {
+  const int c0 = (t & 127) * 4;
+  const int dst = e_index(c0 & 7, (c0 >> 3) & 7, c0 >> 6);
+#pragma unroll
+  for (int j = 0; j < 7; ++j) {
+    const int k = (t >> 7) + 4 * j;
+    if (k < 27) {
+      float *e = E + k * EPL + dst;
+      e[0] = r.v[j].x; e[1] = r.v[j].y; e[2] = r.v[j].z; e[3] = r.v[j].w;
+    }
+  }
+}
+__device__ __forceinline__ void own_store(const OwnRegs<StoreF16S> &r, float inv_scale, int t,
+                                          float *E) {
+  const int c0 = (t & 63) * 8;
+  const int dst = e_index(0, (c0 >> 3) & 7, c0 >> 6);
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const int k = (t >> 6) + 8 * j;
+    if (k < 27) {
+      const __half2 *h = (const __half2 *)&r.v[j];
+      const float w = w_of(k), sc = w * inv_scale;
+      float *e = E + k * EPL + dst;
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const float2 f2 = __half22float2(h[i]);
+        e[2 * i] = fmaf(f2.x, sc, w);
+        e[2 * i + 1] = fmaf(f2.y, sc, w);
+      }
+    }
+  }
+}
+
+// Halo part of the staging, then the own block's registers into E.
 // ghost_row: this block's precomputed absent-neighbour values in table order
 // (kHaloEntries floats), or null to compute them here with `fill`.
 template <class ST, class FILL>
-__device__ __forceinline__ void stage_block(const void *f_in_v, int64_t dstride, float inv_scale,
-                                            const int *nbbase, int t, float *E,
-                                            const uint32_t *__restrict__ tab, bool any_missing,
-                                            const float *__restrict__ ghost_row, FILL fill) {
+__device__ __forceinline__ void stage_halo(const void *f_in_v, int64_t dstride, float inv_scale,
+                                           const int *nbbase, int t, float *E,
+                                           const uint32_t *__restrict__ tab, bool any_missing,
+                                           const float *__restrict__ ghost_row,
+                                           const OwnRegs<ST> &own_regs, FILL fill) {
   using T = typename ST::T;
   const T *__restrict__ fin = (const T *)f_in_v;
-  const int own = nbbase[13];
   // halo sources: all table entries and source values of this thread in flight at once
   uint32_t te[kHaloPerThread];
 #pragma unroll
   for (int j = 0; j < kHaloPerThread; ++j) {
     const int i = t + j * BCELLS;
     te[j] = i < kHaloEntries ? __ldg(tab + i) : 0xFFFFFFFFu;
-  }
-  if (ST::kBytes == 4) {
-    const int c0 = (t & 127) * 4;
-    const int dst = e_index(c0 & 7, (c0 >> 3) & 7, c0 >> 6);
-#pragma unroll
-    for (int j = 0; j < 7; ++j) {
-      const int k = (t >> 7) + 4 * j;
-      if (k < 27) {
-        const float4 v = __ldg((const float4 *)((const float *)fin + (size_t)k * dstride + own + c0));
-        float *e = E + k * EPL + dst;
-        e[0] = v.x; e[1] = v.y; e[2] = v.z; e[3] = v.w;
-      }
-    }
-  } else {
-    const int c0 = (t & 63) * 8;
-    const int dst = e_index(0, (c0 >> 3) & 7, c0 >> 6);
-#pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      const int k = (t >> 6) + 8 * j;
-      if (k < 27) {
-        const uint4 raw = __ldg((const uint4 *)((const __half *)fin + (size_t)k * dstride + own + c0));
-        const __half2 *h = (const __half2 *)&raw;
-        const float w = w_of(k), sc = w * inv_scale;
-        float *e = E + k * EPL + dst;
-#pragma unroll
-        for (int i = 0; i < 4; ++i) {
-          const float2 f2 = __half22float2(h[i]);
-          e[2 * i] = fmaf(f2.x, sc, w);
-          e[2 * i + 1] = fmaf(f2.y, sc, w);
-        }
-      }
-    }
   }
   float hv[kHaloPerThread];
   int hd[kHaloPerThread];
@@ -744,10 +774,21 @@ __device__ __forceinline__ void stage_block(const void *f_in_v, int64_t dstride,
       }
     }
   }
+  own_store(own_regs, inv_scale, t, E);
 #pragma unroll
   for (int j = 0; j < kHaloPerThread; ++j)
     if (hd[j] >= 0) E[hd[j]] = hv[j];
   if (any_missing && !ghost_row) fill();
+}
+
+template <class ST, class FILL>
+__device__ __forceinline__ void stage_block(const void *f_in_v, int64_t dstride, float inv_scale,
+                                            const int *nbbase, int t, float *E,
+                                            const uint32_t *__restrict__ tab, bool any_missing,
+                                            const float *__restrict__ ghost_row, FILL fill) {
+  OwnRegs<ST> r;
+  own_load(f_in_v, dstride, nbbase[13], t, r);
+  stage_halo<ST>(f_in_v, dstride, inv_scale, nbbase, t, E, tab, any_missing, ghost_row, r, fill);
 }
 
 // Neighbour-table row -> element offsets of the 27 neighbour blocks, then a
@@ -770,6 +811,16 @@ __device__ __forceinline__ void stage_flow(const LevelDev &L, const int *nbbase,
   const float *ghost_row = ghost_row_of(L, b);
   stage_block<ST>(L.f_in, L.dstride, L.inv_scale, nbbase, t, E, L.halo_tab, any_missing,
                   ghost_row, [&]() { fill_missing_flow<ST>(L, nbbase, b, t, E); });
+}
+
+// The same with the own block already in registers (own_load issued before
+// the neighbour table was read).
+template <class ST>
+__device__ __forceinline__ void stage_flow(const LevelDev &L, const int *nbbase, int b, int t,
+                                           float *E, bool any_missing, const OwnRegs<ST> &r) {
+  const float *ghost_row = ghost_row_of(L, b);
+  stage_halo<ST>(L.f_in, L.dstride, L.inv_scale, nbbase, t, E, L.halo_tab, any_missing,
+                 ghost_row, r, [&]() { fill_missing_flow<ST>(L, nbbase, b, t, E); });
 }
 
 // obs / spg: this cell's obstacle flag and sponge weight, loaded by the
