@@ -31,6 +31,7 @@ from __future__ import annotations
 import argparse
 import json
 import os
+import re
 import statistics
 import subprocess
 import sys
@@ -328,15 +329,14 @@ def main():
     alg_bytes = fin.n_blocks * 512 * B_ALG["f32"]
     peak, peak_kind = peaks()
     achieved = alg_bytes / (k_ms / 1e3) / 1e9
+    # DRAM bytes per call of the same finest-level launch, from the committed
+    # ncu summary of this workload (null when there is none)
     traffic = None
-    prof = os.path.join(ROOT, "profiles", "stream_collide_traffic.json")
+    prof = os.path.join(ROOT, "profiles", f"k_stream_collide_{a.workload}_level{len(levels)}.md")
     if os.path.exists(prof):
-        try:
-            with open(prof) as fh:
-                d = json.load(fh)
-            traffic = d.get("bytes_per_launch_scaled", {}).get(a.workload)
-        except Exception:
-            traffic = None
+        with open(prof) as fh:
+            m = re.search(r"^traffic_bytes_per_launch\s*=\s*(\d+)", fh.read(), re.M)
+        traffic = int(m.group(1)) if m else None
 
     # native block-pool path: FP32 and FP16-shifted storage, one CUDA-graph
     # replay per coarse step, timed with events on the context stream
