@@ -109,6 +109,8 @@ def build_case(workload: str):
         cfg, mesh = workloads.cube_3lvl()
     elif workload == "sphere_1lvl":
         cfg, mesh = workloads.sphere_1lvl()
+    elif workload == "sphere_ddf":
+        cfg, mesh = workloads.sphere_ddf()
     else:
         raise SystemExit(f"unknown workload {workload}")
     p = scaling.compute_domain_from_mesh(cfg, mesh.min_bounds, mesh.max_bounds)
@@ -132,7 +134,7 @@ def time_cpu_baseline(cfg, p, hosts, budget_s: float = 15.0) -> dict:
     from openludwig_b200.solver import StepSettings
     st = StepSettings.from_config(cfg, cfg.wall_model_enabled)
     s = odrv.settings_dict(st)
-    lv = odrv.init_levels(hosts)
+    lv = odrv.init_levels(hosts, ddf=bool(cfg.ddf_enabled))
     dims = (p.nx_coarse, p.ny_coarse, p.nz_coarse)
     upd = sum(h.n_blocks * 512 * (1 << i) for i, h in enumerate(hosts))
     t0 = time.perf_counter()
@@ -172,7 +174,7 @@ def main():
         from openludwig_b200.solver import StepSettings
         st = StepSettings.from_config(cfg, cfg.wall_model_enabled)
         s = odrv.settings_dict(st)
-        lv = odrv.init_levels(hosts)
+        lv = odrv.init_levels(hosts, ddf=bool(cfg.ddf_enabled))
         dims = (p.nx_coarse, p.ny_coarse, p.nz_coarse)
         upd = sum(h.n_blocks * 512 * (1 << i) for i, h in enumerate(hosts))
         # bounded sample per step: one coarse step of the workload
@@ -210,7 +212,7 @@ def main():
 
     cfg, mesh, p, hosts = build_case(a.workload)
     dev = torch.device("cuda", local)
-    levels = [S.upload_level(h, dev) for h in hosts]
+    levels = [S.upload_level(h, dev, ddf=bool(cfg.ddf_enabled)) for h in hosts]
     st = S.StepSettings.from_config(cfg, cfg.wall_model_enabled)
     dims = (p.nx_coarse, p.ny_coarse, p.nz_coarse)
     u = float(cfg.u_target)
@@ -344,10 +346,12 @@ def main():
     case = NT.PreparedCase(cfg, mesh, p, hosts, st)
     native = {}
     for storage in ("f32", "f16"):
-        probe = NT.Context(device=local, budget_bytes=64 << 20, storage=storage)
+        ddf = bool(cfg.ddf_enabled)
+        probe = NT.Context(device=local, budget_bytes=64 << 20, storage=storage, ddf=ddf)
         need = probe.footprint(case)
         probe.close()
-        ctx = NT.Context(device=local, budget_bytes=int(need * 1.25) + (64 << 20), storage=storage)
+        ctx = NT.Context(device=local, budget_bytes=int(need * 1.25) + (64 << 20), storage=storage,
+                         ddf=ddf)
         cid = ctx.add_case(case)
         ctx.step(a.warmup)
         ctx.sync()

@@ -313,6 +313,34 @@ OL_API int ol_ctx_autotune(ol_ctx *ctx, int32_t trials);
 OL_API int ol_ctx_stats(ol_ctx *ctx, size_t *used, size_t *budget, int32_t *n_cases,
                  int64_t *launches);
 
+/* ------------------------------------------------------------------------
+ * Domain preprocessing on the device (the host build is the reference's
+ * CPU path; these give the same bits).  All pointers are device memory:
+ *   coords   [n_blocks][3] 1-based block coordinates (x, y, z) of the level
+ *   tris     [n_tris][3][3] triangle vertices (mesh frame, FP64)
+ *   tri_off  [n_blocks + 1], tri_list: per block, ascending 0-based ids of
+ *            the triangles whose bounding box (+ margin) touches the block
+ *   offset   host array, the mesh offset added to every vertex
+ * ------------------------------------------------------------------------ */
+/* Solid cells: some triangle overlaps the cell's box of half size
+ * 0.75 dx * 1.001 (separating axes).  Replaces voxelize_blocks!
+ * (domain_generation.jl:74-112 with the test of :10-32; margin 2 dx).
+ * obstacle [512 n_blocks], 1 = solid (before the flood fill). */
+OL_API int ol_voxelize(const int32_t *coords, int32_t n_blocks, const double *tris,
+                       int32_t n_tris, const int32_t *tri_off, const int32_t *tri_list,
+                       double dx, const double offset[3], uint8_t *obstacle, void *stream);
+/* Bouzidi wall distances: per cell and link the nearest ray hit (Moller-
+ * Trumbore, eps 1e-9) along the unit link direction, q = t / (dx |c_k|) kept
+ * in (0, 1] as binary16 with its 1-based triangle id; has_link marks cells
+ * with at least one kept link.  Replaces compute_bouzidi_qmap_sparse
+ * (bouzidi_setup.jl:64-166, bouzidi_math.jl:9-101; margin 2.5 dx).
+ * q_map / tri_map [27][512 n_blocks] (column-major [x,y,z,b,k]), has_link
+ * [512 n_blocks]. */
+OL_API int ol_bouzidi_qmap(const int32_t *coords, int32_t n_blocks, const double *tris,
+                           int32_t n_tris, const int32_t *tri_off, const int32_t *tri_list,
+                           double dx, const double offset[3], uint16_t *q_map,
+                           int32_t *tri_map, uint8_t *has_link, void *stream);
+
 /* Message of the last failing call on this thread. */
 OL_API const char *ol_last_error(void);
 /* Library version string. */

@@ -119,6 +119,10 @@ _SIGS = {
     "ol_bouzidi_sparse": (C.c_int, [vp, vp, vp, vp, vp, vp, i32, vp, i32, f32, vp, vp]),
     "ol_bouzidi_sparse_noalloc": (C.c_int, [vp, vp, vp, vp, vp, vp, i32, vp, i32, f32, vp]),
     "ol_thermal": (C.c_int, [C.POINTER(ThermalView), C.POINTER(ThermalParams), vp]),
+    "ol_voxelize": (C.c_int, [vp, i32, vp, i32, vp, vp, C.c_double, C.POINTER(C.c_double), vp,
+                              vp]),
+    "ol_bouzidi_qmap": (C.c_int, [vp, i32, vp, i32, vp, vp, C.c_double, C.POINTER(C.c_double),
+                                  vp, vp, vp, vp]),
     "ol_init_equilibrium": (C.c_int, [vp, vp, vp, vp, vp, i32, vp]),
     "ol_surface_forces": (C.c_int, [C.POINTER(SurfaceMesh), vp, vp, vp, vp, i32,
                                     C.POINTER(ForceParams), vp, vp, vp, vp, vp,

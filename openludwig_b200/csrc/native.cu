@@ -110,7 +110,7 @@ __device__ __forceinline__ void copy_desc(DEV *dst, const DEV *src, int t) {
 // Boundary values of absent neighbours for the ghost blocks of many cases:
 // one CTA per (descriptor, block) item.
 template <class ST>
-__global__ void __launch_bounds__(kGhostThreads)
+__global__ void __launch_bounds__(kGhostThreads, kGhostMinBlocks)
     k_ghost_fill_b(const LevelDev *__restrict__ descs, const WorkItem *__restrict__ items) {
   __shared__ __align__(16) LevelDev L;
   const WorkItem w = items[blockIdx.x];

@@ -549,6 +549,7 @@ __device__ __noinline__ void fill_missing_flow(const LevelDev &L, const int *nbb
 // interpolate.  Parent cell indices are kept as int32 (the launch checks
 // that the parent's cells fit).
 constexpr int kGhostThreads = 256;
+constexpr int kGhostMinBlocks = 4;  // resident CTAs per SM (64 registers per thread)
 constexpr int kGhostScan = (kHaloEntries + kGhostThreads - 1) / kGhostThreads;  // 13
 
 // Warp-aggregated append of `value` to a shared list when `flag` is set;
@@ -670,7 +671,7 @@ __device__ __forceinline__ void ghost_fill_block(const LevelDev &L, int b, float
 
 // Drop-in: one CTA per block of the level (rows indexed by block).
 template <class ST>
-__global__ void __launch_bounds__(kGhostThreads)
+__global__ void __launch_bounds__(kGhostThreads, kGhostMinBlocks)
     k_ghost_fill(const __grid_constant__ LevelDev L) {
   ghost_fill_block<ST>(L, blockIdx.x, L.ghost + (size_t)blockIdx.x * kHaloEntries);
 }

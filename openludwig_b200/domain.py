@@ -447,6 +447,69 @@ def compute_bouzidi_qmap(coords: np.ndarray, tris: np.ndarray, dx: float, offset
     return q16, trim, cells
 
 
+# ------------------------------------------------- the same two steps on a GPU
+
+def _tri_csr(bmap: list) -> tuple[np.ndarray, np.ndarray]:
+    off = np.zeros(len(bmap) + 1, dtype=np.int32)
+    off[1:] = np.cumsum([len(t) for t in bmap])
+    lst = np.fromiter((t for tl in bmap for t in tl), dtype=np.int32, count=int(off[-1]))
+    return off, lst
+
+
+class DeviceGeometry:
+    """Triangles of one mesh resident on a CUDA device, for ol_voxelize and
+    ol_bouzidi_qmap (same bits as voxelize_blocks / compute_bouzidi_qmap)."""
+
+    def __init__(self, tris: np.ndarray, device: int = 0):
+        import torch
+        from . import _native as N
+        self.torch, self.N = torch, N
+        self.dev = torch.device("cuda", device)
+        self.n_tris = int(tris.shape[0])
+        self.tris = torch.from_numpy(np.ascontiguousarray(tris, dtype=np.float64)).to(self.dev)
+
+    def _common(self, coords, bmap, dx, offset):
+        t = self.torch
+        off_arr, lst = _tri_csr(bmap)
+        d_coords = t.from_numpy(np.ascontiguousarray(coords, dtype=np.int32)).to(self.dev)
+        d_off = t.from_numpy(off_arr).to(self.dev)
+        d_lst = t.from_numpy(lst if lst.size else np.zeros(1, np.int32)).to(self.dev)
+        o3 = (self.N.C.c_double * 3)(*[float(v) for v in offset])
+        return d_coords, d_off, d_lst, o3
+
+    def _p(self, a):
+        return self.N.C.c_void_p(a.data_ptr())
+
+    def voxelize(self, coords: np.ndarray, dx: float, offset, bmap: list) -> np.ndarray:
+        n = coords.shape[0]
+        d_coords, d_off, d_lst, o3 = self._common(coords, bmap, dx, offset)
+        out = self.torch.empty(n * 512, dtype=self.torch.uint8, device=self.dev)
+        s = self.N.C.c_void_p(self.torch.cuda.current_stream(self.dev).cuda_stream)
+        self.N.call("ol_voxelize", self._p(d_coords), self.N.i32(n), self._p(self.tris),
+                    self.N.i32(self.n_tris), self._p(d_off), self._p(d_lst), float(dx), o3,
+                    self._p(out), s)
+        return out.cpu().numpy()
+
+    def qmap(self, coords: np.ndarray, dx: float, offset, bmap: list):
+        t = self.torch
+        n = coords.shape[0]
+        S = n * 512
+        d_coords, d_off, d_lst, o3 = self._common(coords, bmap, dx, offset)
+        q = t.empty(S * 27, dtype=t.int16, device=self.dev)
+        tri = t.empty(S * 27, dtype=t.int32, device=self.dev)
+        has = t.empty(S, dtype=t.uint8, device=self.dev)
+        s = self.N.C.c_void_p(t.cuda.current_stream(self.dev).cuda_stream)
+        self.N.call("ol_bouzidi_qmap", self._p(d_coords), self.N.i32(n), self._p(self.tris),
+                    self.N.i32(self.n_tris), self._p(d_off), self._p(d_lst), float(dx), o3,
+                    self._p(q), self._p(tri), self._p(has), s)
+        q16 = q.cpu().numpy().view(np.uint16)
+        trim = tri.cpu().numpy()
+        idx = np.nonzero(has.cpu().numpy())[0]
+        cells = np.stack([idx // 512 + 1, idx % 8 + 1, (idx // 8) % 8 + 1, (idx // 64) % 8 + 1],
+                         axis=1).astype(np.int32).reshape(-1, 4)
+        return q16, trim, cells
+
+
 def should_use_bouzidi(level_id: int, num_levels: int, method: str, bouzidi_levels: int) -> bool:
     """bouzidi_common.jl:28-33."""
     return method == "bouzidi" and level_id > num_levels - bouzidi_levels
@@ -486,10 +549,13 @@ def level_block_set(lvl: int, tris: np.ndarray, dx: float, offset, dims, prev_co
 
 
 def setup_multilevel_domain(cfg: CaseConfig, mesh: SolverMesh, p: DomainParams,
-                            with_bouzidi: bool = True) -> list[HostLevel]:
-    """domain.jl:1-246."""
+                            with_bouzidi: bool = True,
+                            device: int | None = None) -> list[HostLevel]:
+    """domain.jl:1-246.  device: CUDA device for the voxelisation and the
+    Bouzidi q-map (ol_voxelize / ol_bouzidi_qmap, same bits), None = host."""
     tris = mesh.triangles
     offset = p.mesh_offset
+    dg = DeviceGeometry(tris, device) if device is not None else None
     pmin = np.asarray(p.mesh_min) + np.asarray(offset)
     pmax = np.asarray(p.mesh_max) + np.asarray(offset)
     wake_box = None
@@ -511,7 +577,11 @@ def setup_multilevel_domain(cfg: CaseConfig, mesh: SolverMesh, p: DomainParams,
                                  wake_box, cfg)
         table = build_neighbor_table(coords, dims)
         ptr, gdim = block_pointer(coords)
-        obst = voxelize_blocks(coords, tris, dx, offset)
+        if dg is not None:
+            obst = dg.voxelize(coords, dx, offset,
+                               block_triangle_map(tris, coords, dx, offset, dx * 2))
+        else:
+            obst = voxelize_blocks(coords, tris, dx, offset)
         obst = flood_fill(coords, obst)
         sponge = apply_sponge(coords, dx, p.domain_size, cfg.sponge_thickness, cfg.symmetric_analysis)
         wd = (compute_wall_distances(coords, table, obst, dx) if cfg.wall_model_enabled
@@ -523,7 +593,11 @@ def setup_multilevel_domain(cfg: CaseConfig, mesh: SolverMesh, p: DomainParams,
                        sponge=sponge, wall_dist=wd)
         if with_bouzidi and should_use_bouzidi(lvl, p.num_levels, cfg.boundary_method,
                                                cfg.bouzidi_levels):
-            q16, trim, cells = compute_bouzidi_qmap(coords, tris, dx, offset)
+            if dg is not None:
+                q16, trim, cells = dg.qmap(coords, dx, offset,
+                                           block_triangle_map(tris, coords, dx, offset, dx * 2.5))
+            else:
+                q16, trim, cells = compute_bouzidi_qmap(coords, tris, dx, offset)
             if cells.shape[0] > 0:
                 lv.bouzidi = True
                 lv.q_map, lv.tri_map = q16, trim

@@ -51,10 +51,12 @@ class PreparedCase:
         return sum(h.n_blocks * 512 for h in self.levels)
 
 
-def prepare_case(cfg: CaseConfig, mesh: SolverMesh, name: str = "") -> PreparedCase:
-    """Domain scaling + multi-level domain build (host)."""
+def prepare_case(cfg: CaseConfig, mesh: SolverMesh, name: str = "",
+                 device: int | None = None) -> PreparedCase:
+    """Domain scaling + multi-level domain build; device: CUDA device for the
+    voxelisation and Bouzidi q-map (None = all on the host)."""
     p = compute_domain_from_mesh(cfg, mesh.min_bounds, mesh.max_bounds)
-    hosts = setup_multilevel_domain(cfg, mesh, p)
+    hosts = setup_multilevel_domain(cfg, mesh, p, device=device)
     st = StepSettings.from_config(cfg, cfg.wall_model_enabled)
     return PreparedCase(cfg, mesh, p, hosts, st, name)
 
