@@ -74,6 +74,11 @@ def main() -> None:
     if not a.no_serial:
         serial = SV.serial_baseline(cases, storage=a.storage, budget_bytes=budget, **rule)
         line["serial"] = _summary(serial)
+        if a.rate == 0:
+            # every request queued at t = 0: request k completes after cases 0..k
+            done = np.cumsum([r.finish_s for r in serial["results"]])
+            line["serial"]["p50_s"] = float(np.percentile(done, 50))
+            line["serial"]["p99_s"] = float(np.percentile(done, 99))
         line["served_over_serial"] = served["solves_per_hour"] / serial["solves_per_hour"]
     print(json.dumps(line), flush=True)
 
