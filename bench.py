@@ -205,6 +205,7 @@ def main():
     torch.cuda.set_device(local)
     if world > 1:
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    from openludwig_b200 import replicas
     from openludwig_b200 import build as olbuild
     olbuild.build()
     from openludwig_b200 import _native as N
@@ -260,12 +261,8 @@ def main():
             graph.replay()
         e1.record(stream)
     torch.cuda.synchronize()
-    dt_ms = e0.elapsed_time(e1)
-    if world > 1:
-        tt = torch.tensor([dt_ms], device=dev)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        dt_ms = float(tt.item())
-    value = upd * nsteps * world / (dt_ms / 1e3) / 1e6
+    rate, dt_ms = replicas.job_rate(upd * nsteps, e0.elapsed_time(e1), dev)
+    value = rate / 1e6
 
     # e2e: reference-facing C-ABI calls per level sub-step + per-step D2H of diagnostics
     nb = hosts[0].n_blocks
@@ -289,12 +286,8 @@ def main():
                    S._ptr(partials), out7, C.c_void_p(stream.cuda_stream))
         ee1.record(stream)
     torch.cuda.synchronize()
-    e2e_ms = ee0.elapsed_time(ee1)
-    if world > 1:
-        tt = torch.tensor([e2e_ms], device=dev)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        e2e_ms = float(tt.item())
-    e2e = upd * ke * world / (e2e_ms / 1e3) / 1e6
+    e2e_rate, e2e_ms = replicas.job_rate(upd * ke, ee0.elapsed_time(ee1), dev)
+    e2e = e2e_rate / 1e6
     clocks = clk.stop()
     h2d_per_step = launches_per_step * C.sizeof(N.StepParams)
 
@@ -355,8 +348,8 @@ def main():
         cid = ctx.add_case(case)
         ctx.step(a.warmup)
         ctx.sync()
-        ms = ctx.step_timed(nsteps)
-        native[storage] = {"MLUPS": upd * nsteps * world / (ms / 1e3) / 1e6,
+        n_rate, ms = replicas.job_rate(upd * nsteps, ctx.step_timed(nsteps), dev)
+        native[storage] = {"MLUPS": n_rate / 1e6,
                            "ms_per_step": ms / nsteps,
                            "launches_per_step": ctx.stats()["launches"] // max(1, a.warmup + nsteps),
                            "bytes_per_cell_update_alg": B_ALG[storage]}

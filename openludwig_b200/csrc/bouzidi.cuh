@@ -1,5 +1,6 @@
 // Bouzidi interpolated bounce-back on the sparse boundary-cell list
-// (bouzidi_kernel.jl:13-92), one thread per (boundary cell, direction).
+// (bouzidi_kernel.jl:13-92), one thread per (boundary cell, direction),
+// direction-major so that a warp reads neighbouring cells of one plane.
 //
 // For each link k of a boundary cell x with q in (q_min, 1]:
 //   q <  1/2 : f_out[x, opp k] = 2q f*[x,k] + (1-2q) f*[x + c_opp k, k]
@@ -81,8 +82,8 @@ template <class ST>
 __global__ void k_bouzidi_direct(const __grid_constant__ BouzDev B) {
   const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= (int64_t)B.n_boundary * 27) return;
-  const int64_t i = j / 27;
-  const int k = (int)(j - i * 27);
+  const int k = (int)(j / B.n_boundary);  // direction-major: neighbouring threads
+  const int64_t i = j - (int64_t)k * B.n_boundary;  // take neighbouring cells
   size_t own;
   float v;
   if (bouzidi_link<ST>(B, i, k, own, v))
@@ -94,8 +95,8 @@ template <class ST>
 __global__ void k_bouzidi_gather(const __grid_constant__ BouzDev B) {
   const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= (int64_t)B.n_boundary * 27) return;
-  const int64_t i = j / 27;
-  const int k = (int)(j - i * 27);
+  const int k = (int)(j / B.n_boundary);  // direction-major: neighbouring threads
+  const int64_t i = j - (int64_t)k * B.n_boundary;  // take neighbouring cells
   size_t own;
   float v;
   if (bouzidi_link<ST>(B, i, k, own, v)) B.scratch[j] = v;
@@ -106,8 +107,8 @@ template <class ST>
 __global__ void k_bouzidi_scatter(const __grid_constant__ BouzDev B) {
   const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= (int64_t)B.n_boundary * 27) return;
-  const int64_t i = j / 27;
-  const int k = (int)(j - i * 27);
+  const int k = (int)(j / B.n_boundary);  // direction-major: neighbouring threads
+  const int64_t i = j - (int64_t)k * B.n_boundary;  // take neighbouring cells
   const int b = B.cell_block[i] - 1;
   const int x = B.cell_x[i] - 1, y = B.cell_y[i] - 1, z = B.cell_z[i] - 1;
   const size_t own = (size_t)(B.block_offset + b) * BCELLS + x + BS * y + BS * BS * z;

@@ -158,8 +158,9 @@ __global__ void k_bouz_gather_b(const LevelDev *descs, const ThermalDev *tdescs,
                                 float *scratch) {
   const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= n_links) return;
-  const BouzItem it = items[j / 27];
-  const int k = (int)(j % 27);
+  const int64_t n_items = n_links / 27;  // direction-major: neighbouring threads
+  const int k = (int)(j / n_items);        // take neighbouring boundary cells
+  const BouzItem it = items[j - (int64_t)k * n_items];
   BouzDev B = bd[it.bdesc];
   void *f = B.thermal ? tdescs[B.desc].g_out : descs[B.desc].f_out;
   B.f = f;
@@ -175,8 +176,9 @@ __global__ void k_bouz_scatter_b(const LevelDev *descs, const ThermalDev *tdescs
                                  const float *scratch) {
   const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= n_links) return;
-  const BouzItem it = items[j / 27];
-  const int k = (int)(j % 27);
+  const int64_t n_items = n_links / 27;  // direction-major: neighbouring threads
+  const int k = (int)(j / n_items);        // take neighbouring boundary cells
+  const BouzItem it = items[j - (int64_t)k * n_items];
   const BouzDev &B = bd[it.bdesc];
   void *f = B.thermal ? tdescs[B.desc].g_out : descs[B.desc].f_out;
   const int i = it.cell;

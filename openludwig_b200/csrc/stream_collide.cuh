@@ -52,14 +52,49 @@ __device__ __forceinline__ void parent_stencil(const LevelDev &L, int gx, int gy
   }
 }
 
+// a * (1 - w) + b * w, each product and the sum rounded on its own (as the
+// reference's Float32 expression; the same bits wherever it is evaluated)
+__device__ __forceinline__ float lerp_rn(float a, float b, float w) {
+  return __fadd_rn(__fmul_rn(a, __fsub_rn(1.0f, w)), __fmul_rn(b, w));
+}
+
 __device__ __forceinline__ float trilerp(const float (&v)[8], float wx, float wy, float wz) {
-  const float c00 = v[0] * (1.0f - wx) + v[1] * wx;
-  const float c01 = v[4] * (1.0f - wx) + v[5] * wx;
-  const float c10 = v[2] * (1.0f - wx) + v[3] * wx;
-  const float c11 = v[6] * (1.0f - wx) + v[7] * wx;
-  const float c0 = c00 * (1.0f - wy) + c10 * wy;
-  const float c1 = c01 * (1.0f - wy) + c11 * wy;
-  return c0 * (1.0f - wz) + c1 * wz;
+  const float c00 = lerp_rn(v[0], v[1], wx);
+  const float c01 = lerp_rn(v[4], v[5], wx);
+  const float c10 = lerp_rn(v[2], v[3], wx);
+  const float c11 = lerp_rn(v[6], v[7], wx);
+  const float c0 = lerp_rn(c00, c10, wy);
+  const float c1 = lerp_rn(c01, c11, wy);
+  return lerp_rn(c0, c1, wz);
+}
+
+// Blended parent moments (rho, ux, uy, uz) of the present parent cell c.
+__device__ __forceinline__ void corner_moments(const LevelDev &L, int64_t c, float (&m)[4]) {
+  const ol_step_params &sp = L.sp;
+  const bool temporal = sp.use_temporal_interp == 1 && sp.temporal_weight < 0.99f;
+  const float tw = sp.temporal_weight;
+  const float rn = L.prho[c], uxn = L.pvel[c], uyn = L.pvel[c + L.p_dstride],
+              uzn = L.pvel[c + 2 * L.p_dstride];
+  if (temporal) {
+    m[0] = lerp_rn(L.prho_old[c], rn, tw);
+    m[1] = lerp_rn(L.pvel_old[c], uxn, tw);
+    m[2] = lerp_rn(L.pvel_old[c + L.p_dstride], uyn, tw);
+    m[3] = lerp_rn(L.pvel_old[c + 2 * L.p_dstride], uzn, tw);
+  } else {
+    m[0] = rn; m[1] = uxn; m[2] = uyn; m[3] = uzn;
+  }
+}
+
+// Blended parent population k of the present parent cell c.
+template <class ST>
+__device__ __forceinline__ float corner_population(const LevelDev &L, int64_t c, int k) {
+  const ol_step_params &sp = L.sp;
+  const bool temporal = sp.use_temporal_interp == 1 && sp.temporal_weight < 0.99f;
+  const size_t a = (size_t)c + (size_t)k * L.p_dstride;
+  const float fn = ST::load((const typename ST::T *)L.pf, a, k, L.p_inv_scale);
+  return temporal ? lerp_rn(ST::load((const typename ST::T *)L.pf_old, a, k, L.p_inv_scale), fn,
+                            sp.temporal_weight)
+                  : fn;
 }
 
 // Parent rho, ux, uy, uz at the ghost position: each corner blended between
@@ -67,28 +102,13 @@ __device__ __forceinline__ float trilerp(const float (&v)[8], float wx, float wy
 // missing, then rho = 1, u = 0) first corner, then trilinear.
 __device__ __forceinline__ void interp_moments(const LevelDev &L, const ParentStencil &P,
                                                float (&r)[4]) {
-  const ol_step_params &sp = L.sp;
-  const bool temporal = sp.use_temporal_interp == 1 && sp.temporal_weight < 0.99f;
-  const float tw = sp.temporal_weight;
   float v[4][8];
 #pragma unroll
   for (int s = 0; s < 8; ++s) {
-    v[0][s] = 1.0f; v[1][s] = 0.0f; v[2][s] = 0.0f; v[3][s] = 0.0f;
-    const int64_t c = P.ci[s];
-    if (c >= 0) {
-      const float rn = L.prho[c], uxn = L.pvel[c], uyn = L.pvel[c + L.p_dstride],
-                  uzn = L.pvel[c + 2 * L.p_dstride];
-      if (temporal) {
-        const float ro = L.prho_old[c], uxo = L.pvel_old[c], uyo = L.pvel_old[c + L.p_dstride],
-                    uzo = L.pvel_old[c + 2 * L.p_dstride];
-        v[0][s] = ro * (1.0f - tw) + rn * tw;
-        v[1][s] = uxo * (1.0f - tw) + uxn * tw;
-        v[2][s] = uyo * (1.0f - tw) + uyn * tw;
-        v[3][s] = uzo * (1.0f - tw) + uzn * tw;
-      } else {
-        v[0][s] = rn; v[1][s] = uxn; v[2][s] = uyn; v[3][s] = uzn;
-      }
-    }
+    float m[4] = {1.0f, 0.0f, 0.0f, 0.0f};
+    if (P.ci[s] >= 0) corner_moments(L, P.ci[s], m);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) v[i][s] = m[i];
   }
 #pragma unroll
   for (int s = 1; s < 8; ++s)
@@ -99,39 +119,34 @@ __device__ __forceinline__ void interp_moments(const LevelDev &L, const ParentSt
   for (int i = 0; i < 4; ++i) r[i] = trilerp(v[i], P.wx, P.wy, P.wz);
 }
 
-// Ghost population k: interpolated f_k split into equilibrium (from the
-// interpolated moments r) and non-equilibrium part, the latter rescaled by
-// (tau_f - 1/2) / (tau_c - 1/2) clamped to [0.01, 100].
-template <class ST>
-__device__ __forceinline__ float interp_population(const LevelDev &L, int k,
-                                                   const ParentStencil &P, const float (&r)[4]) {
+// From the 8 corner values of f_k (absent corners already replaced): the
+// interpolated f_k split into equilibrium (from the interpolated moments r)
+// and non-equilibrium part, the latter rescaled by (tau_f - 1/2) /
+// (tau_c - 1/2) clamped to [0.01, 100].
+__device__ __forceinline__ float finish_population(const LevelDev &L, int k, const float (&v)[8],
+                                                   float wx, float wy, float wz,
+                                                   const float (&r)[4]) {
   const ol_step_params &sp = L.sp;
-  const bool temporal = sp.use_temporal_interp == 1 && sp.temporal_weight < 0.99f;
-  const float tw = sp.temporal_weight;
-  const float w = w_of(k);
-  const typename ST::T *pf = (const typename ST::T *)L.pf;
-  const typename ST::T *pfo = (const typename ST::T *)L.pf_old;
-  float v[8];
-#pragma unroll
-  for (int s = 0; s < 8; ++s) {
-    v[s] = w;
-    const int64_t c = P.ci[s];
-    if (c >= 0) {
-      const size_t a = (size_t)c + (size_t)k * L.p_dstride;
-      const float fn = ST::load(pf, a, k, L.p_inv_scale);
-      v[s] = temporal ? ST::load(pfo, a, k, L.p_inv_scale) * (1.0f - tw) + fn * tw : fn;
-    }
-  }
-#pragma unroll
-  for (int s = 1; s < 8; ++s)
-    if (P.ci[s] < 0) v[s] = v[0];
-  const float fi = trilerp(v, P.wx, P.wy, P.wz);
-  const float fe = feq_auto(r[0], r[1], r[2], r[3], w, (float)cx_of(k), (float)cy_of(k),
+  const float fi = trilerp(v, wx, wy, wz);
+  const float fe = feq_auto(r[0], r[1], r[2], r[3], w_of(k), (float)cx_of(k), (float)cy_of(k),
                             (float)cz_of(k), sp.compressible_corr);
   const float fneq = fi - fe;
   const float tc = sp.tau_parent - 0.5f, tf = sp.tau_molecular - 0.5f;
   const float sc = tc > 1e-6f ? fminf(fmaxf(tf / tc, 0.01f), 100.0f) : 1.0f;
-  return fe + fneq * sc;
+  return __fadd_rn(fe, __fmul_rn(fneq, sc));
+}
+
+// Ghost population k at a position with stencil P and moments r.
+template <class ST>
+__device__ __forceinline__ float interp_population(const LevelDev &L, int k,
+                                                   const ParentStencil &P, const float (&r)[4]) {
+  float v[8];
+#pragma unroll
+  for (int s = 0; s < 8; ++s) v[s] = P.ci[s] >= 0 ? corner_population<ST>(L, P.ci[s], k) : w_of(k);
+#pragma unroll
+  for (int s = 1; s < 8; ++s)
+    if (P.ci[s] < 0) v[s] = v[0];
+  return finish_population(L, k, v, P.wx, P.wy, P.wz, r);
 }
 
 // ---------------------------------------------------------------------------
@@ -984,10 +999,15 @@ __device__ __forceinline__ void collide_cell(const LevelDev &L, const int *nbbas
       A[k] = A[k] + g * ft;
     }
   }
+  if (fpost) {
 #pragma unroll
-  for (int k = 0; k < 27; ++k) {
-    ST::store(fout, own + (size_t)k * L.dstride, k, L.scale, A[k]);
-    if (fpost) fpost[own + (size_t)k * L.dstride] = A[k];
+    for (int k = 0; k < 27; ++k) {
+      ST::store(fout, own + (size_t)k * L.dstride, k, L.scale, A[k]);
+      fpost[own + (size_t)k * L.dstride] = A[k];
+    }
+  } else {
+#pragma unroll
+    for (int k = 0; k < 27; ++k) ST::store(fout, own + (size_t)k * L.dstride, k, L.scale, A[k]);
   }
 }
 
