@@ -36,8 +36,10 @@ struct StoreF16S {
   }
   __device__ __forceinline__ static void store(T *p, size_t i, int k,
                                                float scale, float v) {
+    // scale * (1/w) with the reciprocal folded at compile time: the same
+    // bits as scale / w for the power-of-two scales the layer uses
     const float w = w_of(k);
-    p[i] = __float2half_rn((v - w) * (scale / w));
+    p[i] = __float2half_rn((v - w) * (scale * (1.0f / w)));
   }
 };
 
