@@ -313,6 +313,28 @@ OL_API int ol_ctx_autotune(ol_ctx *ctx, int32_t trials);
 OL_API int ol_ctx_stats(ol_ctx *ctx, size_t *used, size_t *budget, int32_t *n_cases,
                  int64_t *launches);
 
+/* Fine-to-coarse restriction, opt-in; no counterpart in the reference, whose
+ * levels are coupled coarse to fine only (physics_interpolation.jl).  After a
+ * parent step and its two child sub-steps, every parent cell covered by a
+ * child block gets the average of its 8 children: fbar = mean f, rho and u
+ * from fbar, f = feq(rho, u) + (fbar - feq) * clamp((tau_c - 1/2) /
+ * (tau_f - 1/2), 0.01, 100); rho and u are stored.  Parent cells that are
+ * solid or have a solid child are left alone.  Column-major reference layout. */
+typedef struct ol_restrict_view {
+  const float *f_fine;              /* [512*nF*27] child's newest populations  */
+  const uint8_t *obstacle_fine;     /* [512*nF]                                 */
+  const int32_t *map_x, *map_y, *map_z; /* [nF] child block coordinates        */
+  int32_t n_fine;
+  float *f_coarse;                  /* [512*nC*27] parent's newest, updated     */
+  float *rho_coarse, *vel_coarse;   /* [512*nC], [512*nC*3], updated            */
+  const uint8_t *obstacle_coarse;   /* [512*nC]                                 */
+  const int32_t *block_ptr;         /* parent block pointer grid                */
+  int32_t dim_x, dim_y, dim_z, n_coarse;
+  float tau_fine, tau_coarse;
+  int32_t compressible;             /* O(u^4) equilibrium when nonzero          */
+} ol_restrict_view;
+OL_API int ol_restrict(const ol_restrict_view *v, void *stream);
+
 /* ------------------------------------------------------------------------
  * Domain preprocessing on the device (the host build is the reference's
  * CPU path; these give the same bits).  All pointers are device memory:

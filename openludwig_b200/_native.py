@@ -70,6 +70,14 @@ class ThermalParams(C.Structure):
     _fields_ = THERMAL_FIELDS
 
 
+class RestrictView(C.Structure):
+    _fields_ = [("f_fine", vp), ("obstacle_fine", vp), ("map_x", vp), ("map_y", vp),
+                ("map_z", vp), ("n_fine", i32), ("f_coarse", vp), ("rho_coarse", vp),
+                ("vel_coarse", vp), ("obstacle_coarse", vp), ("block_ptr", vp), ("dim_x", i32),
+                ("dim_y", i32), ("dim_z", i32), ("n_coarse", i32), ("tau_fine", f32),
+                ("tau_coarse", f32), ("compressible", i32)]
+
+
 class SurfaceMesh(C.Structure):
     _fields_ = [("cx", vp), ("cy", vp), ("cz", vp), ("nx", vp), ("ny", vp), ("nz", vp),
                 ("area", vp), ("n_triangles", i32)]
@@ -119,6 +127,7 @@ _SIGS = {
     "ol_bouzidi_sparse": (C.c_int, [vp, vp, vp, vp, vp, vp, i32, vp, i32, f32, vp, vp]),
     "ol_bouzidi_sparse_noalloc": (C.c_int, [vp, vp, vp, vp, vp, vp, i32, vp, i32, f32, vp]),
     "ol_thermal": (C.c_int, [C.POINTER(ThermalView), C.POINTER(ThermalParams), vp]),
+    "ol_restrict": (C.c_int, [C.POINTER(RestrictView), vp]),
     "ol_voxelize": (C.c_int, [vp, i32, vp, i32, vp, vp, C.c_double, C.POINTER(C.c_double), vp,
                               vp]),
     "ol_bouzidi_qmap": (C.c_int, [vp, i32, vp, i32, vp, vp, C.c_double, C.POINTER(C.c_double),

@@ -80,6 +80,7 @@ class CaseConfig:
     nu_sgs_background: float = f32(0.0)
     sponge_blend_distributions: bool = False
     temporal_interpolation: bool = True
+    fine_to_coarse_restriction: bool = False   # opt-in extension, not in the reference
     cumulant_omega_bulk: float = f32(1.0)
     cumulant_omega_3: float = f32(1.0)
     cumulant_omega_4: float = f32(1.0)
@@ -182,6 +183,7 @@ def config_from_dict(cfg: dict, case_dir: str = ".") -> CaseConfig:
     c.nu_sgs_background = f32(g("nu_sgs_background", d=0.0))
     c.sponge_blend_distributions = bool(g("sponge_blend_distributions", d=False))
     c.temporal_interpolation = bool(g("temporal_interpolation", d=True))
+    c.fine_to_coarse_restriction = bool(g("fine_to_coarse_restriction", d=False))
     c.cumulant_omega_bulk = f32(g("cumulant", "omega_bulk", d=1.0))
     c.cumulant_omega_3 = f32(g("cumulant", "omega_3", d=1.0))
     c.cumulant_omega_4 = f32(g("cumulant", "omega_4", d=1.0))

@@ -177,6 +177,9 @@ class StepSettings:
     t_inlet: float = 1.0
     t_wall: float = 1.0
     wall_bc_adiabatic: int = 1
+    # fine-to-coarse restriction after each pair of child sub-steps (opt-in;
+    # the reference couples the levels coarse to fine only)
+    restriction: int = 0
 
     @staticmethod
     def from_config(cfg: CaseConfig, wall_model_active: bool) -> "StepSettings":
@@ -192,7 +195,8 @@ class StepSettings:
                             compressible=int(cfg.compressibility_correction),
                             q_min=cfg.q_min_threshold, ddf=int(cfg.ddf_enabled),
                             t_inlet=cfg.ddf_t_inlet, t_wall=cfg.ddf_t_wall,
-                            wall_bc_adiabatic=int(cfg.ddf_wall_bc == "adiabatic"))
+                            wall_bc_adiabatic=int(cfg.ddf_wall_bc == "adiabatic"),
+                            restriction=int(cfg.fine_to_coarse_restriction))
 
 
 def step_params(s: StepSettings, lv: DeviceLevel, parent_tau: float, is_l1: bool, dims, u: float,
@@ -325,6 +329,24 @@ def recursive_step(levels: list, s: StepSettings, lvl: int, t_sub: int, parent: 
         me = ParentRef(lv, f_out, vel_out, g_out if s.ddf else None)
         recursive_step(levels, s, lvl + 1, 2 * t_sub, me, 0.0, u, domain_dims)
         recursive_step(levels, s, lvl + 1, 2 * t_sub + 1, me, 0.5, u, domain_dims)
+        if s.restriction:
+            # the child's second sub-step (odd t_sub) wrote f and vel
+            restrict_level(levels[lvl + 1], me, s)
+
+
+def restrict_level(child: DeviceLevel, parent: ParentRef, s: StepSettings) -> None:
+    """Fine-to-coarse restriction (ol_restrict) of the child's newest state
+    into the parent's newest state; an opt-in extension of the reference."""
+    p = parent.lv
+    d = p.host.grid_dim
+    v = N.RestrictView(f_fine=_ptr(child.f), obstacle_fine=_ptr(child.obstacle),
+                       map_x=_ptr(child.map_x), map_y=_ptr(child.map_y), map_z=_ptr(child.map_z),
+                       n_fine=child.n_blocks, f_coarse=_ptr(parent.f_new), rho_coarse=_ptr(p.rho),
+                       vel_coarse=_ptr(parent.vel_new), obstacle_coarse=_ptr(p.obstacle),
+                       block_ptr=_ptr(p.block_ptr), dim_x=d[0], dim_y=d[1], dim_z=d[2],
+                       n_coarse=p.n_blocks, tau_fine=child.tau, tau_coarse=p.tau,
+                       compressible=s.compressible)
+    N.call("ol_restrict", C.byref(v), _stream())
 
 
 def execute_timestep_batch(levels, s: StepSettings, t_start: int, batch: int, u: float,

@@ -147,6 +147,11 @@ def recursive_step(levels, s, lvl, t_sub, parent, tw, u, domain_dims, dtype):
                   tau=h.tau, tau_g=h.tau_g, g=g_out, T=lv.T, g_old=lv.g_old, T_old=lv.T_old)
         recursive_step(levels, s, lvl + 1, 2 * t_sub, me, 0.0, u, domain_dims, dtype)
         recursive_step(levels, s, lvl + 1, 2 * t_sub + 1, me, 0.5, u, domain_dims, dtype)
+        if s.get("restriction"):
+            c = levels[lvl + 1]   # its second sub-step (odd t_sub) wrote f and vel
+            orc.restrict(c.f, c.host.obstacle, c.host.map_x, c.host.map_y, c.host.map_z,
+                         c.host.n_blocks, f_out, lv.rho, vel_out, h.obstacle, h.block_ptr,
+                         h.grid_dim, h.n_blocks, c.host.tau, h.tau, s["compressible_corr"], dtype)
 
 
 def settings_dict(st) -> dict:
@@ -158,4 +163,5 @@ def settings_dict(st) -> dict:
                 omega_3=st.omega_3, omega_4=st.omega_4, adaptive_omega4=st.adaptive_omega4,
                 lambda_param=st.lambda_param, limiter_type=st.limiter,
                 compressible_corr=st.compressible, q_min=st.q_min, ddf=st.ddf,
-                T_inlet=st.t_inlet, T_wall=st.t_wall, wall_bc_adiabatic=st.wall_bc_adiabatic)
+                T_inlet=st.t_inlet, T_wall=st.t_wall, wall_bc_adiabatic=st.wall_bc_adiabatic,
+                restriction=st.restriction)

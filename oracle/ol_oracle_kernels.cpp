@@ -833,6 +833,70 @@ void orc_bouzidi_f64(double *f_out, const double *f_post, const uint16_t *q, con
   bouzidi(f_out, f_post, q, cb, cx, cy, cz, n, nbr, nB, qmin);
 }
 
+// Fine-to-coarse restriction, the opt-in extension of this package (no
+// reference counterpart): each coarse cell covered by a fine block takes the
+// average of its 8 children, non-equilibrium part rescaled by
+// clamp((tau_c - 1/2) / (tau_f - 1/2), 0.01, 100); solid cells are skipped.
+#define ORC_RESTRICT_BODY(R)                                                                  \
+  const size_t fS = (size_t)nF * NC, cS = (size_t)nC * NC;                                   \
+  for (int fb = 0; fb < nF; ++fb)                                                             \
+    for (int q = 0; q < 64; ++q) {                                                            \
+      const int i = q & 3, j = (q >> 2) & 3, l = q >> 4;                                      \
+      const int gx = (mx[fb] - 1) * 4 + i + 1, gy = (my[fb] - 1) * 4 + j + 1,                \
+                gz = (mz[fb] - 1) * 4 + l + 1;                                                \
+      const int bx = (gx - 1) / 8 + 1, by = (gy - 1) / 8 + 1, bz = (gz - 1) / 8 + 1;          \
+      if (bx > dx || by > dy || bz > dz) continue;                                            \
+      const int pb = bptr[(bx - 1) + dx * ((by - 1) + dy * (bz - 1))];                        \
+      if (pb <= 0) continue;                                                                  \
+      const size_t cc = (size_t)(pb - 1) * NC + (gx - 1) % 8 + 8 * ((gy - 1) % 8) +           \
+                        64 * ((gz - 1) % 8);                                                  \
+      if (obs_c[cc]) continue;                                                                \
+      size_t fc[8];                                                                           \
+      bool solid = false;                                                                     \
+      for (int s = 0; s < 8; ++s) {                                                           \
+        fc[s] = (size_t)fb * NC + (2 * i + (s & 1)) + 8 * (2 * j + ((s >> 1) & 1)) +          \
+                64 * (2 * l + (s >> 2));                                                      \
+        solid = solid || obs_f[fc[s]];                                                        \
+      }                                                                                       \
+      if (solid) continue;                                                                    \
+      R fbar[27], rho = 0, jx = 0, jy = 0, jz = 0;                                            \
+      for (int k = 0; k < 27; ++k) {                                                          \
+        R acc = 0;                                                                            \
+        for (int s = 0; s < 8; ++s) acc = acc + f_f[fc[s] + k * fS];                          \
+        fbar[k] = acc * (R)0.125;                                                             \
+      }                                                                                       \
+      for (int k = 0; k < 27; ++k) {                                                          \
+        rho = rho + fbar[k];                                                                  \
+        if (LAT.cx[k] == 1) jx = jx + fbar[k]; else if (LAT.cx[k] == -1) jx = jx - fbar[k];   \
+        if (LAT.cy[k] == 1) jy = jy + fbar[k]; else if (LAT.cy[k] == -1) jy = jy - fbar[k];   \
+        if (LAT.cz[k] == 1) jz = jz + fbar[k]; else if (LAT.cz[k] == -1) jz = jz - fbar[k];   \
+      }                                                                                       \
+      const R ux = jx / rho, uy = jy / rho, uz = jz / rho;                                    \
+      const R tf = (R)tau_f - (R)0.5, tc = (R)tau_c - (R)0.5;                                 \
+      const R sc = tf > (R)1e-6f ? rclamp(tc / tf, (R)0.01f, (R)100.0f) : (R)1;               \
+      for (int k = 0; k < 27; ++k) {                                                          \
+        const R fe = feq_auto(rho, ux, uy, uz, wk<R>(k), (R)LAT.cx[k], (R)LAT.cy[k],          \
+                              (R)LAT.cz[k], comp);                                            \
+        f_c[cc + k * cS] = fe + (fbar[k] - fe) * sc;                                          \
+      }                                                                                       \
+      rho_c[cc] = rho;                                                                        \
+      vel_c[cc] = ux; vel_c[cc + cS] = uy; vel_c[cc + 2 * cS] = uz;                           \
+    }
+
+void orc_restrict_f32(const float *f_f, const uint8_t *obs_f, const int32_t *mx,
+                      const int32_t *my, const int32_t *mz, int32_t nF, float *f_c, float *rho_c,
+                      float *vel_c, const uint8_t *obs_c, const int32_t *bptr, int32_t dx,
+                      int32_t dy, int32_t dz, int32_t nC, float tau_f, float tau_c, int32_t comp) {
+  ORC_RESTRICT_BODY(float)
+}
+void orc_restrict_f64(const double *f_f, const uint8_t *obs_f, const int32_t *mx,
+                      const int32_t *my, const int32_t *mz, int32_t nF, double *f_c,
+                      double *rho_c, double *vel_c, const uint8_t *obs_c, const int32_t *bptr,
+                      int32_t dx, int32_t dy, int32_t dz, int32_t nC, float tau_f, float tau_c,
+                      int32_t comp) {
+  ORC_RESTRICT_BODY(double)
+}
+
 #define ORC_THERMAL_ARGS(R)                                                                   \
   R *g_out, const R *g_in, R *g_post, R *T_out, const R *vel, const uint8_t *obs,             \
       const float *sponge, const int32_t *nbr, const int32_t *mx, const int32_t *my,          \

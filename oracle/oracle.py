@@ -91,6 +91,16 @@ def bouzidi(f_out, f_post, q_map, cell_block, cx, cy, cz, neighbor_table, n_bloc
        C.c_int32(len(cell_block)), _p(neighbor_table), C.c_int32(n_blocks), C.c_float(q_min))
 
 
+def restrict(f_f, obs_f, mx, my, mz, n_f, f_c, rho_c, vel_c, obs_c, block_ptr, dims, n_c,
+             tau_f, tau_c, compressible, dtype=np.float32) -> None:
+    """Fine-to-coarse restriction in place on the coarse arrays (ol_restrict)."""
+    fn = lib().orc_restrict_f32 if dtype == np.float32 else lib().orc_restrict_f64
+    fn.restype = None
+    fn(_p(f_f), _p(obs_f), _p(mx), _p(my), _p(mz), C.c_int32(n_f), _p(f_c), _p(rho_c), _p(vel_c),
+       _p(obs_c), _p(block_ptr), C.c_int32(dims[0]), C.c_int32(dims[1]), C.c_int32(dims[2]),
+       C.c_int32(n_c), C.c_float(tau_f), C.c_float(tau_c), C.c_int32(int(compressible)))
+
+
 def thermal(tv: dict, pv: dict | None, params: dict, dtype=np.float32) -> None:
     fn = lib().orc_thermal_f32 if dtype == np.float32 else lib().orc_thermal_f64
     tp = _fill(ThermalParamsC, params)

@@ -12,7 +12,7 @@ import ctypes as C
 import numpy as np
 import pytest
 
-from helpers import max_abs, perturbed_state, rel_err, small_sphere_case
+from helpers import max_abs, perturbed_state, rel_err, small_sphere_case, weights32
 
 pytestmark = pytest.mark.gpu
 
@@ -184,6 +184,48 @@ def test_ghost_pass_equals_inline_fill():
         assert la.ghost is not None and lb.ghost is None
         assert torch.equal(la.f_temp, lb.f_temp) and torch.equal(la.f, lb.f)
         assert torch.equal(la.vel_temp, lb.vel_temp) and torch.equal(la.rho, lb.rho)
+
+
+def test_restriction_matches_oracle():
+    """Opt-in fine-to-coarse restriction: one ol_restrict call against the
+    oracle on a perturbed state, then 20 coarse steps of a two-level case
+    with restriction on against the oracle recursion."""
+    c, mesh, p, hosts = small_sphere_case(resolution=16, levels=2, c_wale=np.float32(0.5))
+    hc, hf = hosts
+    rng = np.random.default_rng(4)
+    w = weights32()
+    f_f = (np.repeat(w, 512 * hf.n_blocks) * rng.uniform(0.95, 1.05, 27 * 512 * hf.n_blocks)
+           ).astype(np.float32)
+    f_c = (np.repeat(w, 512 * hc.n_blocks) * rng.uniform(0.95, 1.05, 27 * 512 * hc.n_blocks)
+           ).astype(np.float32)
+    rho_c = np.ones(512 * hc.n_blocks, np.float32)
+    vel_c = np.zeros(3 * 512 * hc.n_blocks, np.float32)
+    d = {k: _t(v) for k, v in dict(f_f=f_f, f_c=f_c, rho_c=rho_c, vel_c=vel_c,
+                                     of=hf.obstacle, oc=hc.obstacle, mx=hf.map_x, my=hf.map_y,
+                                     mz=hf.map_z, bp=hc.block_ptr).items()}
+    v = N.RestrictView(f_fine=S._ptr(d["f_f"]), obstacle_fine=S._ptr(d["of"]),
+                       map_x=S._ptr(d["mx"]), map_y=S._ptr(d["my"]), map_z=S._ptr(d["mz"]),
+                       n_fine=hf.n_blocks, f_coarse=S._ptr(d["f_c"]), rho_coarse=S._ptr(d["rho_c"]),
+                       vel_coarse=S._ptr(d["vel_c"]), obstacle_coarse=S._ptr(d["oc"]),
+                       block_ptr=S._ptr(d["bp"]), dim_x=hc.grid_dim[0], dim_y=hc.grid_dim[1],
+                       dim_z=hc.grid_dim[2], n_coarse=hc.n_blocks, tau_fine=hf.tau,
+                       tau_coarse=hc.tau, compressible=0)
+    N.call("ol_restrict", C.byref(v), S._stream())
+    torch.cuda.synchronize()
+    orc.restrict(f_f, hf.obstacle, hf.map_x, hf.map_y, hf.map_z, hf.n_blocks, f_c, rho_c, vel_c,
+                 hc.obstacle, hc.block_ptr, hc.grid_dim, hc.n_blocks, hf.tau, hc.tau, 0)
+    g = d["f_c"].cpu().numpy()
+    assert max_abs(g, f_c) < 1e-6
+    assert not np.array_equal(g, np.repeat(w, 512 * hc.n_blocks))  # cells were replaced
+    assert max_abs(d["rho_c"].cpu().numpy(), rho_c) < 1e-6
+    # the recursion with restriction on
+    st = S.StepSettings.from_config(c, False)
+    st.restriction = 1
+    gl = _run_gpu(hosts, p, st, 20, 0.05)
+    ol = _run_oracle(hosts, p, st, 20, 0.05)
+    for lg, lo in zip(gl, ol):
+        assert rel_err(lg.f_temp.cpu().numpy(), lo.f_temp) < 1e-4
+        assert rel_err(lg.rho.cpu().numpy(), lo.rho) < 1e-5
 
 
 def test_two_level_thermal_ddf():

@@ -123,3 +123,55 @@ def test_bouzidi_special_q(q, expect):
                                     rel=1e-6)
     changed = np.nonzero(f_out != f_post)[0]
     assert set(changed.tolist()) <= {cell + ko * 512}
+
+
+def _restrict_setup(f_fine, dtype):
+    """One parent block (coords 1,1,1) fully covered by two child blocks."""
+    mx = np.array([1, 2], np.int32)
+    my = np.array([1, 1], np.int32)
+    mz = np.array([1, 1], np.int32)
+    f_c = np.repeat(np.asarray(weights32(), dtype), 512).astype(dtype)
+    rho_c = np.ones(512, dtype)
+    vel_c = np.zeros(3 * 512, dtype)
+    orc.restrict(f_fine, np.zeros(2 * 512, np.uint8), mx, my, mz, 2, f_c, rho_c, vel_c,
+                 np.zeros(512, np.uint8), np.array([1], np.int32), (1, 1, 1), 1,
+                 0.53, 0.56, 0, dtype)
+    return f_c, rho_c, vel_c
+
+
+def test_restriction_keeps_equilibrium_and_conserves_mass_momentum():
+    """Fine-to-coarse restriction (opt-in extension): an equilibrium state is
+    a fixed point, and the restricted cell keeps the children's mean mass and
+    momentum (the non-equilibrium rescaling adds neither)."""
+    cx, cy, cz = lattice()
+    w = weights32().astype(np.float64)
+    rho, ux, uy, uz = 1.02, 0.05, -0.01, 0.02
+    cu = cx * ux + cy * uy + cz * uz
+    feq = rho * w * (1 + 3 * cu + 4.5 * cu * cu - 1.5 * (ux * ux + uy * uy + uz * uz))
+    f_c, rho_c, vel_c = _restrict_setup(np.repeat(feq, 2 * 512), np.float64)
+    # the children cover parent cells x = 0..7, y = 0..3, z = 0..3
+    covered = [x + 8 * y + 64 * z for z in range(4) for y in range(4) for x in range(8)]
+    F_c = f_c.reshape(27, 512)
+    for c in covered:
+        np.testing.assert_allclose(F_c[:, c], feq, rtol=1e-12)
+    untouched = 7 + 8 * 7 + 64 * 7
+    np.testing.assert_array_equal(F_c[:, untouched], w)
+    assert rho_c[0] == pytest.approx(feq.sum(), rel=1e-12)       # FP32 weights: sum != 1 exactly
+    assert vel_c[0] == pytest.approx((feq * cx).sum() / feq.sum(), rel=1e-12)
+    # random children: mean mass and momentum kept
+    rng = np.random.default_rng(11)
+    f_f = (np.repeat(w, 2 * 512) * rng.uniform(0.9, 1.1, 27 * 2 * 512)).astype(np.float64)
+    f_c, rho_c, vel_c = _restrict_setup(f_f, np.float64)
+    F = f_f.reshape(27, 2 * 512)
+    for c in (0, 9, 63, 200, 511):
+        x, y, z = c % 8, (c // 8) % 8, c // 64
+        fb, lx = divmod(x, 4)
+        kids = [fb * 512 + (2 * lx + a) + 8 * (2 * y % 8 + b) + 64 * (2 * z % 8 + d)
+                for d in (0, 1) for b in (0, 1) for a in (0, 1)] if y < 4 and z < 4 else None
+        if kids is None:
+            continue
+        mean = F[:, kids].mean(axis=1)
+        got = f_c.reshape(27, 512)[:, c]
+        assert got.sum() == pytest.approx(mean.sum(), rel=1e-12)
+        assert (got * cx).sum() == pytest.approx((mean * cx).sum(), abs=1e-12)
+        assert (got * cz).sum() == pytest.approx((mean * cz).sum(), abs=1e-12)
