@@ -171,6 +171,9 @@ typedef struct ol_thermal_view {
   /* parent (coarse-to-fine, physics_interpolation.jl:135-247) */
   const float *pg, *pT, *pvel, *pg_old, *pT_old, *pvel_old;
   const int32_t *p_block_ptr; int32_t p_dim_x, p_dim_y, p_dim_z, p_n_blocks;
+  /* optional [ol_ghost_floats(nB)] scratch, as ol_level_view.ghost: the
+   * boundary values of absent neighbours by a separate pass (same results) */
+  float *ghost;
 } ol_thermal_view;
 
 typedef struct ol_thermal_params {

@@ -55,7 +55,7 @@ class ThermalView(C.Structure):
                 ("map_y", vp), ("map_z", vp), ("n_blocks", i32),
                 ("pg", vp), ("pT", vp), ("pvel", vp), ("pg_old", vp), ("pT_old", vp),
                 ("pvel_old", vp), ("p_block_ptr", vp), ("p_dim_x", i32), ("p_dim_y", i32),
-                ("p_dim_z", i32), ("p_n_blocks", i32)]
+                ("p_dim_z", i32), ("p_n_blocks", i32), ("ghost", vp)]
 
 
 THERMAL_FIELDS = [("tau_g", f32), ("tau_g_parent", f32), ("is_level_1", i32),

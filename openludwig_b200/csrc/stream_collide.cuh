@@ -24,7 +24,8 @@ struct ParentStencil {
   float wx, wy, wz;  // trilinear weights
 };
 
-__device__ __forceinline__ void parent_stencil(const LevelDev &L, int gx, int gy, int gz,
+template <class DEV>
+__device__ __forceinline__ void parent_stencil(const DEV &L, int gx, int gy, int gz,
                                                ParentStencil &P) {
   const float pxc = ((float)gx - 0.5f) * 0.5f;
   const float pyc = ((float)gy - 0.5f) * 0.5f;
@@ -580,16 +581,36 @@ __device__ __forceinline__ void append_if(bool flag, int value, int *count, int1
 }
 
 // Row of block b in the ghost scratch of level L (null when the block has
-// no row: no scratch, or no absent neighbour under a compact index).
-__device__ __forceinline__ float *ghost_row_of(const LevelDev &L, int b) {
+// no row: no scratch, or no absent neighbour under a compact index).  DEV is
+// the flow (LevelDev) or thermal (ThermalDev) level.
+template <class DEV>
+__device__ __forceinline__ float *ghost_row_of(const DEV &L, int b) {
   if (!L.ghost) return nullptr;
   const int r = L.gidx ? L.gidx[b] : b;
   return r >= 0 ? L.ghost + (size_t)r * kHaloEntries : nullptr;
 }
 
-// One CTA of kGhostThreads threads evaluates block b's row G.
+// What the ghost pass needs to know of a flow level; the thermal DDF
+// provides the same four functions for its populations (thermal.cuh).
+__device__ __forceinline__ const ol_step_params &ghost_params(const LevelDev &L) { return L.sp; }
+__device__ __forceinline__ void ghost_moments(const LevelDev &L, const ParentStencil &P,
+                                              float (&r)[4]) {
+  interp_moments(L, P, r);
+}
 template <class ST>
-__device__ __forceinline__ void ghost_fill_block(const LevelDev &L, int b, float *G) {
+__device__ __forceinline__ float ghost_population(const LevelDev &L, int k, const ParentStencil &P,
+                                                  const float (&r)[4], ST) {
+  return interp_population<ST>(L, k, P, r);
+}
+template <class ST>
+__device__ __forceinline__ float ghost_boundary(const LevelDev &L, int k, int b, int x, int y,
+                                                int z, ST) {
+  return pull_boundary<ST>(L, k, b, x, y, z);
+}
+
+// One CTA of kGhostThreads threads evaluates block b's row G.
+template <class ST, class DEV>
+__device__ __forceinline__ void ghost_fill_block(const DEV &L, int b, float *G) {
   __shared__ int nbbase[27];
   __shared__ int n_pos, n_slot;
   __shared__ float rs[4][kRingEntries];     // interpolated rho, ux, uy, uz
@@ -607,7 +628,7 @@ __device__ __forceinline__ void ghost_fill_block(const LevelDev &L, int b, float
   }
   if (t == 0) { n_pos = 0; n_slot = 0; }
   if (!__syncthreads_or(missing)) return;
-  const ol_step_params &sp = L.sp;
+  const auto &sp = ghost_params(L);
   const uint32_t *__restrict__ tab = L.halo_tab;
   const bool fine = sp.is_level_1 == 0;
   const int gx0 = (L.map_x[b] - 1) * BS + 1, gy0 = (L.map_y[b] - 1) * BS + 1,
@@ -654,7 +675,7 @@ __device__ __forceinline__ void ghost_fill_block(const LevelDev &L, int b, float
       ParentStencil P;
       parent_stencil(L, gx0 + sx, gy0 + sy, gz0 + sz, P);
       float r[4];
-      interp_moments(L, P, r);
+      ghost_moments(L, P, r);
 #pragma unroll
       for (int i = 0; i < 4; ++i) rs[i][q] = r[i];
 #pragma unroll
@@ -676,9 +697,9 @@ __device__ __forceinline__ void ghost_fill_block(const LevelDev &L, int b, float
       for (int s = 0; s < 8; ++s) P.ci[s] = cs[s][q];
       P.wx = ws[0][q]; P.wy = ws[1][q]; P.wz = ws[2][q];
       const float r[4] = {rs[0][q], rs[1][q], rs[2][q], rs[3][q]};
-      v = interp_population<ST>(L, k, P, r);
+      v = ghost_population(L, k, P, r, ST{});
     } else {
-      v = pull_boundary<ST>(L, k, b, sx + cx_of(k), sy + cy_of(k), sz + cz_of(k));
+      v = ghost_boundary(L, k, b, sx + cx_of(k), sy + cy_of(k), sz + cz_of(k), ST{});
     }
     G[i] = v;
   }

@@ -15,6 +15,14 @@ __global__ void __launch_bounds__(512, 2) k_thermal(const __grid_constant__ Ther
   thermal_cell<ST>(D, nbbase, E, b, threadIdx.x);
 }
 
+// Boundary values of the absent-neighbour thermal pulls of every block, into
+// D.ghost (the flow's ghost pass for the thermal populations).
+template <class ST>
+__global__ void __launch_bounds__(kGhostThreads, kGhostMinBlocks)
+    k_ghost_fill_thermal(const __grid_constant__ ThermalDev D) {
+  ghost_fill_block<ST>(D, blockIdx.x, D.ghost + (size_t)blockIdx.x * kHaloEntries);
+}
+
 template <class ST>
 static void launch_t(const ThermalDev &D, cudaStream_t s) {
   static bool done = false;
@@ -22,6 +30,7 @@ static void launch_t(const ThermalDev &D, cudaStream_t s) {
     cudaFuncSetAttribute(k_thermal<ST>, cudaFuncAttributeMaxDynamicSharedMemorySize, kStageBytes);
     done = true;
   }
+  if (D.ghost) k_ghost_fill_thermal<ST><<<D.n_blocks, kGhostThreads, 0, s>>>(D);
   k_thermal<ST><<<D.n_blocks, BCELLS, kStageBytes, s>>>(D);
 }
 
@@ -54,6 +63,7 @@ extern "C" int ol_thermal(const ol_thermal_view *tv, const ol_thermal_params *tp
   D.dstride = (int64_t)BCELLS * tv->n_blocks;
   D.nbr_stride = tv->n_blocks;
   D.scale = 1.0f; D.inv_scale = 1.0f; D.p_inv_scale = 1.0f;
+  D.ghost = tv->ghost;
   D.tp = *tp;
   D.halo_tab = halo_table_device();
   if (!D.halo_tab) return set_error(OL_ERR_CUDA, "ol_thermal: staging table allocation failed");

@@ -20,84 +20,89 @@ struct ThermalDev {
   float p_inv_scale;
   ol_thermal_params tp;
   const uint32_t *halo_tab;
+  float *ghost;            // absent-neighbour pull sources, kHaloEntries per row, or null
+  const int32_t *gidx;     // block -> ghost row (-1: none); null = row b for block b
 };
 
-// Coarse-to-fine thermal ghost (physics_interpolation.jl:135-247).
-template <class ST>
-__device__ __noinline__ float interp_parent_thermal(const ThermalDev &D, int k, int gx,
-                                                    int gy, int gz) {
+// Coarse-to-fine thermal ghost (physics_interpolation.jl:135-247), in the
+// parts the ghost pass shares with the flow (stream_collide.cuh): blended
+// corner moments (T, u), the blended corner population g_k, trilinear
+// weights, then g = g_eq(T, u) + (g - g_eq) * clamp((tau_g - 1/2) /
+// (tau_g,parent - 1/2), 0.01, 100).
+__device__ __forceinline__ const ol_thermal_params &ghost_params(const ThermalDev &D) {
+  return D.tp;
+}
+__device__ __forceinline__ void ghost_moments(const ThermalDev &D, const ParentStencil &P,
+                                              float (&r)[4]) {
   const ol_thermal_params &tp = D.tp;
-  const float w = w_of(k);
-  const float cx = (float)cx_of(k), cy = (float)cy_of(k), cz = (float)cz_of(k);
-  const float pxc = ((float)gx - 0.5f) * 0.5f;
-  const float pyc = ((float)gy - 0.5f) * 0.5f;
-  const float pzc = ((float)gz - 0.5f) * 0.5f;
-  int px0 = (int)floorf(pxc), py0 = (int)floorf(pyc), pz0 = (int)floorf(pzc);
-  const int px1 = px0 + 1, py1 = py0 + 1, pz1 = pz0 + 1;
-  const float wx = pxc - (float)px0, wy = pyc - (float)py0, wz = pzc - (float)pz0;
-  px0 = max(1, px0); py0 = max(1, py0); pz0 = max(1, pz0);
   const bool temporal = tp.use_temporal_interp == 1 && tp.temporal_weight < 0.99f;
   const float tw = tp.temporal_weight;
-  float v[8][5];
-  bool ok[8];
+  float v[4][8];
 #pragma unroll
   for (int s = 0; s < 8; ++s) {
-    const int pgx = (s & 1) ? px1 : px0;
-    const int pgy = (s & 2) ? py1 : py0;
-    const int pgz = (s & 4) ? pz1 : pz0;
-    const int pbx = (pgx - 1) / BS + 1, pby = (pgy - 1) / BS + 1, pbz = (pgz - 1) / BS + 1;
-    ok[s] = false;
-    v[s][0] = w; v[s][1] = 1.0f; v[s][2] = 0.0f; v[s][3] = 0.0f; v[s][4] = 0.0f;
-    if (pbx >= 1 && pbx <= D.pdim_x && pby >= 1 && pby <= D.pdim_y && pbz >= 1 &&
-        pbz <= D.pdim_z) {
-      const int pb = D.pptr[(pbx - 1) + D.pdim_x * ((pby - 1) + D.pdim_y * (pbz - 1))];
-      if (pb > 0) {
-        const int cell = (pgx - 1) % BS + BS * ((pgy - 1) % BS) + BS * BS * ((pgz - 1) % BS);
-        const size_t ci = (size_t)(D.p_block_offset + pb - 1) * BCELLS + cell;
-        const float gn = ST::load((const typename ST::T *)D.pg, ci + (size_t)k * D.p_dstride, k,
-                                  D.p_inv_scale);
-        const float Tn = D.pT[ci];
-        const float uxn = D.pvel[ci], uyn = D.pvel[ci + D.p_dstride],
-                    uzn = D.pvel[ci + 2 * D.p_dstride];
-        if (temporal) {
-          const float go = ST::load((const typename ST::T *)D.pg_old,
-                                    ci + (size_t)k * D.p_dstride, k, D.p_inv_scale);
-          const float To = D.pT_old[ci];
-          const float uxo = D.pvel_old[ci], uyo = D.pvel_old[ci + D.p_dstride],
-                      uzo = D.pvel_old[ci + 2 * D.p_dstride];
-          v[s][0] = go * (1.0f - tw) + gn * tw;
-          v[s][1] = To * (1.0f - tw) + Tn * tw;
-          v[s][2] = uxo * (1.0f - tw) + uxn * tw;
-          v[s][3] = uyo * (1.0f - tw) + uyn * tw;
-          v[s][4] = uzo * (1.0f - tw) + uzn * tw;
-        } else {
-          v[s][0] = gn; v[s][1] = Tn; v[s][2] = uxn; v[s][3] = uyn; v[s][4] = uzn;
-        }
-        ok[s] = true;
+    v[0][s] = 1.0f; v[1][s] = 0.0f; v[2][s] = 0.0f; v[3][s] = 0.0f;
+    const int64_t c = P.ci[s];
+    if (c >= 0) {
+      const float Tn = D.pT[c], uxn = D.pvel[c], uyn = D.pvel[c + D.p_dstride],
+                  uzn = D.pvel[c + 2 * D.p_dstride];
+      if (temporal) {
+        v[0][s] = lerp_rn(D.pT_old[c], Tn, tw);
+        v[1][s] = lerp_rn(D.pvel_old[c], uxn, tw);
+        v[2][s] = lerp_rn(D.pvel_old[c + D.p_dstride], uyn, tw);
+        v[3][s] = lerp_rn(D.pvel_old[c + 2 * D.p_dstride], uzn, tw);
+      } else {
+        v[0][s] = Tn; v[1][s] = uxn; v[2][s] = uyn; v[3][s] = uzn;
       }
     }
   }
 #pragma unroll
   for (int s = 1; s < 8; ++s)
-    if (!ok[s])
+    if (P.ci[s] < 0)
 #pragma unroll
-      for (int i = 0; i < 5; ++i) v[s][i] = v[0][i];
-  float r[5];
+      for (int i = 0; i < 4; ++i) v[i][s] = v[i][0];
 #pragma unroll
-  for (int i = 0; i < 5; ++i) {
-    const float c00 = v[0][i] * (1.0f - wx) + v[1][i] * wx;
-    const float c01 = v[4][i] * (1.0f - wx) + v[5][i] * wx;
-    const float c10 = v[2][i] * (1.0f - wx) + v[3][i] * wx;
-    const float c11 = v[6][i] * (1.0f - wx) + v[7][i] * wx;
-    const float c0 = c00 * (1.0f - wy) + c10 * wy;
-    const float c1 = c01 * (1.0f - wy) + c11 * wy;
-    r[i] = c0 * (1.0f - wz) + c1 * wz;
+  for (int i = 0; i < 4; ++i) r[i] = trilerp(v[i], P.wx, P.wy, P.wz);
+}
+template <class ST>
+__device__ __forceinline__ float ghost_population(const ThermalDev &D, int k,
+                                                  const ParentStencil &P, const float (&r)[4],
+                                                  ST) {
+  const ol_thermal_params &tp = D.tp;
+  const bool temporal = tp.use_temporal_interp == 1 && tp.temporal_weight < 0.99f;
+  const float w = w_of(k);
+  float v[8];
+#pragma unroll
+  for (int s = 0; s < 8; ++s) {
+    v[s] = w;
+    const int64_t c = P.ci[s];
+    if (c >= 0) {
+      const size_t a = (size_t)c + (size_t)k * D.p_dstride;
+      const float gn = ST::load((const typename ST::T *)D.pg, a, k, D.p_inv_scale);
+      v[s] = temporal ? lerp_rn(ST::load((const typename ST::T *)D.pg_old, a, k, D.p_inv_scale),
+                                gn, tp.temporal_weight)
+                      : gn;
+    }
   }
-  const float ge = geq(r[1], r[2], r[3], r[4], w, cx, cy, cz);
-  const float gneq = r[0] - ge;
+#pragma unroll
+  for (int s = 1; s < 8; ++s)
+    if (P.ci[s] < 0) v[s] = v[0];
+  const float gi = trilerp(v, P.wx, P.wy, P.wz);
+  const float ge = geq(r[0], r[1], r[2], r[3], w, (float)cx_of(k), (float)cy_of(k),
+                       (float)cz_of(k));
+  const float gneq = gi - ge;
   const float tc = tp.tau_g_parent - 0.5f, tf = tp.tau_g - 0.5f;
   const float sc = tc > 1e-6f ? fminf(fmaxf(tf / tc, 0.01f), 100.0f) : 1.0f;
-  return ge + gneq * sc;
+  return __fadd_rn(ge, __fmul_rn(gneq, sc));
+}
+
+template <class ST>
+__device__ __noinline__ float interp_parent_thermal(const ThermalDev &D, int k, int gx,
+                                                    int gy, int gz) {
+  ParentStencil P;
+  parent_stencil(D, gx, gy, gz, P);
+  float r[4];
+  ghost_moments(D, P, r);
+  return ghost_population(D, k, P, r, ST{});
 }
 
 // kernel_thermal.jl:90-130
@@ -128,12 +133,19 @@ __device__ __noinline__ float pull_boundary_thermal(const ThermalDev &D, int k, 
   return w * tp.T_inlet;
 }
 
+template <class ST>
+__device__ __forceinline__ float ghost_boundary(const ThermalDev &D, int k, int b, int x, int y,
+                                                int z, ST) {
+  return pull_boundary_thermal<ST>(D, k, b, x, y, z);
+}
+
 // Stage the thermal populations of block b (same layout as the flow).
 template <class ST>
 __device__ __forceinline__ void stage_thermal(const ThermalDev &D, const int *nbbase, int b, int t,
                                               float *E, const uint32_t *tab, bool any_missing) {
   const ThermalDev *Dp = &D;
-  stage_block<ST>(D.g_in, D.dstride, D.inv_scale, nbbase, t, E, tab, any_missing, nullptr, [&]() {
+  stage_block<ST>(D.g_in, D.dstride, D.inv_scale, nbbase, t, E, tab, any_missing,
+                  ghost_row_of(D, b), [&]() {
     fill_missing_slots(nbbase, t, E, tab, [Dp, b](int k, int x, int y, int z) {
       return pull_boundary_thermal<ST>(*Dp, k, b, x, y, z);
     });

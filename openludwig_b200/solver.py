@@ -69,6 +69,7 @@ class DeviceLevel:
     f_post: torch.Tensor | None = None
     # absent-neighbour pull sources, precomputed by a separate pass (optional)
     ghost: torch.Tensor | None = None
+    ghost_g: torch.Tensor | None = None   # the same for the thermal populations
     # thermal DDF
     g: torch.Tensor | None = None
     g_temp: torch.Tensor | None = None
@@ -134,6 +135,8 @@ def upload_level(h: HostLevel, device: torch.device, ddf: bool = False, t_init: 
         lv.ghost = torch.empty(int(N.lib().ol_ghost_floats(N.i32(n))), dtype=torch.float32,
                                device=dev)
     if ddf:
+        if ghost:
+            lv.ghost_g = torch.empty_like(lv.ghost)
         w = torch.tensor(lattice_weights(), dtype=torch.float32, device=dev)
         lv.g = (w[:, None] * t_init).expand(27, S).reshape(-1).clone()
         lv.g_temp = lv.g.clone()
@@ -285,7 +288,8 @@ def perform_timestep(s: StepSettings, lv: DeviceLevel, parent: ParentRef | None,
                            temperature=_ptr(lv.temperature), vel=_ptr(vel_out),
                            obstacle=_ptr(lv.obstacle), sponge=_ptr(lv.sponge),
                            neighbor_table=_ptr(lv.neighbor_table), map_x=_ptr(lv.map_x),
-                           map_y=_ptr(lv.map_y), map_z=_ptr(lv.map_z), n_blocks=n)
+                           map_y=_ptr(lv.map_y), map_z=_ptr(lv.map_z), n_blocks=n,
+                           ghost=_ptr(lv.ghost_g))
         if parent is not None:
             p = parent.lv
             d = p.host.grid_dim

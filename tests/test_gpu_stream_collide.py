@@ -173,17 +173,26 @@ def test_two_level_recursion():
         assert rel_err(lg.rho.cpu().numpy(), lo.rho) < 1e-5
 
 
-def test_ghost_pass_equals_inline_fill():
+@pytest.mark.parametrize("ddf", [False, True], ids=["flow", "flow_thermal"])
+def test_ghost_pass_equals_inline_fill(ddf):
     """Interface and domain-boundary values from the separate pass (ghost
-    scratch) and from the in-staging fill give the same bits."""
-    c, mesh, p, hosts = small_sphere_case(resolution=16, levels=2, c_wale=np.float32(0.5))
+    scratch) and from the in-staging fill give the same bits, for the flow
+    and for the thermal populations."""
+    kw = dict(compressibility_correction=True, ddf_enabled=True,
+              u_target=np.float32(0.1)) if ddf else {}
+    c, mesh, p, hosts = small_sphere_case(resolution=16, levels=2, c_wale=np.float32(0.5), **kw)
     st = S.StepSettings.from_config(c, False)
-    a = _run_gpu(hosts, p, st, 6, 0.05, ghost=True)
-    b = _run_gpu(hosts, p, st, 6, 0.05, ghost=False)
+    u = 0.1 if ddf else 0.05
+    a = _run_gpu(hosts, p, st, 6, u, ddf=ddf, ghost=True)
+    b = _run_gpu(hosts, p, st, 6, u, ddf=ddf, ghost=False)
     for la, lb in zip(a, b):
         assert la.ghost is not None and lb.ghost is None
         assert torch.equal(la.f_temp, lb.f_temp) and torch.equal(la.f, lb.f)
         assert torch.equal(la.vel_temp, lb.vel_temp) and torch.equal(la.rho, lb.rho)
+        if ddf:
+            assert la.ghost_g is not None
+            assert torch.equal(la.g_temp, lb.g_temp) and torch.equal(la.g, lb.g)
+            assert torch.equal(la.temperature, lb.temperature)
 
 
 def test_restriction_matches_oracle():
