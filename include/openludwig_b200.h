@@ -227,6 +227,28 @@ OL_API int ol_surface_forces(const ol_surface_mesh *mesh, const float *rho,
                       double out[9], void *stream);
 OL_API size_t ol_surface_forces_scratch_doubles(int32_t n_triangles);
 
+/* Outputs of ol_surface_net_forces: device arrays of n_triangles floats.
+ * The plus maps are force_data.pressure_map / shear_{x,y,z}_map, the minus
+ * maps force_data.*_map_minus; each side's four are all given or all NULL. */
+typedef struct ol_net_force_maps {
+  float *p_plus, *sx_plus, *sy_plus, *sz_plus;
+  float *p_minus, *sx_minus, *sy_minus, *sz_minus;
+  float *net_fx, *net_fy, *net_fz;       /* per-triangle net force, required */
+} ol_net_force_maps;
+
+/* Two-sided per-triangle net force, replaces compute_net_aerodynamics!
+ * (surface.jl:980-1034) with its kernels map_stresses_kernel! (:350-507),
+ * map_minus_side_only_kernel! (:511-662) and
+ * compute_net_triangle_forces_kernel! (:665-700):
+ * net = -(p+ - p-) n A + (tau+ - tau-) A.  closed_body != 0 zeroes the minus
+ * side without probing it (the reference's default).  One launch on `stream`,
+ * asynchronous; results stay on the device. */
+OL_API int ol_surface_net_forces(const ol_surface_mesh *mesh, const float *rho,
+                          const float *vel, const uint8_t *obstacle,
+                          const int32_t *block_ptr, int32_t n_blocks,
+                          const ol_force_params *fp, int32_t closed_body,
+                          const ol_net_force_maps *out, void *stream);
+
 /* Flow statistics of a level in FP64 (diagnostics.jl:43-93):
  * out[0..6] = {n_fluid, rho_sum, rho_min, rho_max, v_max, kinetic_energy,
  * mass_all_cells}.  `partials` >= ol_flow_stats_scratch_doubles(nB). */
@@ -306,6 +328,10 @@ OL_API int ol_ctx_case_forces(ol_ctx *ctx, int32_t case_id, double out[9]);
  * populations (host [512*nB*27] FP32, decoded), or NULL to skip. */
 OL_API int ol_ctx_case_download(ol_ctx *ctx, int32_t case_id, int32_t level,
                          float *rho, float *vel, float *f);
+/* The same for the thermal DDF of a DDF case: temperature [512*nB] and g
+ * [27][512*nB] (decoded to FP32), either may be NULL. */
+OL_API int ol_ctx_case_download_thermal(ol_ctx *ctx, int32_t case_id, int32_t level,
+                                 float *temperature, float *g);
 /* Coarse steps a case has done, and its device watchdog status. */
 OL_API int ol_ctx_case_info(ol_ctx *ctx, int32_t case_id, int64_t *coarse_steps,
                      int32_t *status);

@@ -83,6 +83,12 @@ class SurfaceMesh(C.Structure):
                 ("area", vp), ("n_triangles", i32)]
 
 
+class NetForceMaps(C.Structure):
+    _fields_ = [("p_plus", vp), ("sx_plus", vp), ("sy_plus", vp), ("sz_plus", vp),
+                ("p_minus", vp), ("sx_minus", vp), ("sy_minus", vp), ("sz_minus", vp),
+                ("net_fx", vp), ("net_fy", vp), ("net_fz", vp)]
+
+
 class ForceParams(C.Structure):
     _fields_ = [("dx", f32), ("dim_x", i32), ("dim_y", i32), ("dim_z", i32),
                 ("offset_x", f32), ("offset_y", f32), ("offset_z", f32),
@@ -137,6 +143,9 @@ _SIGS = {
                                     C.POINTER(ForceParams), vp, vp, vp, vp, vp,
                                     C.POINTER(C.c_double), vp]),
     "ol_surface_forces_scratch_doubles": (C.c_size_t, [i32]),
+    "ol_surface_net_forces": (C.c_int, [C.POINTER(SurfaceMesh), vp, vp, vp, vp, i32,
+                                        C.POINTER(ForceParams), i32, C.POINTER(NetForceMaps),
+                                        vp]),
     "ol_flow_stats": (C.c_int, [vp, vp, vp, i32, vp, C.POINTER(C.c_double), vp]),
     "ol_flow_stats_scratch_doubles": (C.c_size_t, [i32]),
     "ol_ghost_floats": (C.c_int64, [i32]),
@@ -150,6 +159,7 @@ _SIGS = {
     "ol_ctx_step_timed": (C.c_int, [vp, i32, C.POINTER(C.c_float)]),
     "ol_ctx_case_forces": (C.c_int, [vp, i32, C.POINTER(C.c_double)]),
     "ol_ctx_case_download": (C.c_int, [vp, i32, i32, vp, vp, vp]),
+    "ol_ctx_case_download_thermal": (C.c_int, [vp, i32, i32, vp, vp]),
     "ol_ctx_case_info": (C.c_int, [vp, i32, C.POINTER(C.c_int64), C.POINTER(i32)]),
     "ol_ctx_autotune": (C.c_int, [vp, i32]),
     "ol_ctx_stats": (C.c_int, [vp, C.POINTER(C.c_size_t), C.POINTER(C.c_size_t),

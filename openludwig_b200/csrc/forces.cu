@@ -82,6 +82,67 @@ __device__ void stress_from_cell(const ol_force_params &fp, float rho, float ux,
   }
 }
 
+// Flow sample on one side of a triangle centred at t with normal n.
+// SIDE = +1: map_stresses_kernel! (surface.jl:380-483) -- ray-march along +n
+// from 1.5 cells, first sample with fluid weight >= 0.5 wins, else the best
+// one; failing that the nearest fluid cell with dot(c - t, n) > 0, shell by
+// shell.  SIDE = -1: map_minus_side_only_kernel! (surface.jl:545-640) -- the
+// same along -n, accepting dot < 0 with wall distance |dot| / dx.
+template <int SIDE>
+__device__ bool probe_side(const ForceDev &D, float tx, float ty, float tz, float nx, float ny,
+                           float nz, float &br, float &bux, float &buy, float &buz, float &bd) {
+  const ol_force_params &fp = D.fp;
+  const float dx = fp.dx;
+  br = 1.0f; bux = buy = buz = 0.f; bd = 1.0f;
+  float bq = 0.0f;
+  bool found = false;
+  for (int pi = 1; pi <= fp.search_radius; ++pi) {
+    const float dc = (float)pi + 0.5f;
+    float px, py, pz;
+    if constexpr (SIDE > 0) {
+      px = tx + nx * dc * dx; py = ty + ny * dc * dx; pz = tz + nz * dc * dx;
+    } else {
+      px = tx - nx * dc * dx; py = ty - ny * dc * dx; pz = tz - nz * dc * dx;
+    }
+    float r, ux, uy, uz, wq;
+    const bool ok = trilinear_sample(D, px, py, pz, r, ux, uy, uz, wq);
+    if (ok && wq >= 0.5f) {
+      br = r; bux = ux; buy = uy; buz = uz; bd = dc; bq = wq; found = true;
+      break;
+    } else if (ok && wq > bq) {
+      br = r; bux = ux; buy = uy; buz = uz; bd = dc; bq = wq; found = true;
+    }
+  }
+  if (found) return true;
+  const int gx0 = (int)floorf(tx / dx) + 1, gy0 = (int)floorf(ty / dx) + 1,
+            gz0 = (int)floorf(tz / dx) + 1;
+  float best = 1e10f;
+  for (int rad = 1; rad <= fp.search_radius && !found; ++rad) {
+    for (int dz = -rad; dz <= rad; ++dz)
+      for (int dy = -rad; dy <= rad; ++dy)
+        for (int ddx = -rad; ddx <= rad; ++ddx) {
+          if (!(abs(ddx) == rad || abs(dy) == rad || abs(dz) == rad)) continue;
+          const int gx = gx0 + ddx, gy = gy0 + dy, gz = gz0 + dz;
+          size_t ci;
+          if (!cell_at(D, gx, gy, gz, ci) || D.obstacle[ci]) continue;
+          const float ddxp = ((float)gx - 0.5f) * dx - tx;
+          const float ddyp = ((float)gy - 0.5f) * dx - ty;
+          const float ddzp = ((float)gz - 0.5f) * dx - tz;
+          const float dn = ddxp * nx + ddyp * ny + ddzp * nz;
+          if (SIDE > 0 ? dn <= 0.0f : dn >= 0.0f) continue;
+          const float d2 = ddxp * ddxp + ddyp * ddyp + ddzp * ddzp;
+          if (d2 < best) {
+            best = d2;
+            br = D.rho[ci];
+            bux = D.vel[ci]; buy = D.vel[ci + D.dstride]; buz = D.vel[ci + 2 * D.dstride];
+            bd = (SIDE > 0 ? dn : fabsf(dn)) / dx;
+            found = true;
+          }
+        }
+  }
+  return found;
+}
+
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
@@ -95,53 +156,11 @@ __global__ void __launch_bounds__(kForceThreads) k_surface_forces(const __grid_c
   double c[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
   if (i < D.mesh.n_triangles) {
     const ol_force_params &fp = D.fp;
-    const float dx = fp.dx;
     const float tx = D.mesh.cx[i] + fp.offset_x, ty = D.mesh.cy[i] + fp.offset_y,
                 tz = D.mesh.cz[i] + fp.offset_z;
     const float nx = D.mesh.nx[i], ny = D.mesh.ny[i], nz = D.mesh.nz[i];
-    float br = 1.0f, bux = 0.f, buy = 0.f, buz = 0.f, bd = 1.0f, bq = 0.0f;
-    bool found = false;
-    for (int pi = 1; pi <= fp.search_radius; ++pi) {
-      const float dc = (float)pi + 0.5f;
-      float r, ux, uy, uz, wq;
-      const bool ok = trilinear_sample(D, tx + nx * dc * dx, ty + ny * dc * dx,
-                                       tz + nz * dc * dx, r, ux, uy, uz, wq);
-      if (ok && wq >= 0.5f) {
-        br = r; bux = ux; buy = uy; buz = uz; bd = dc; bq = wq; found = true;
-        break;
-      } else if (ok && wq > bq) {
-        br = r; bux = ux; buy = uy; buz = uz; bd = dc; bq = wq; found = true;
-      }
-    }
-    if (!found) {
-      // nearest fluid cell on the + side, shell by shell (surface.jl:423-483)
-      const int gx0 = (int)floorf(tx / dx) + 1, gy0 = (int)floorf(ty / dx) + 1,
-                gz0 = (int)floorf(tz / dx) + 1;
-      float best = 1e10f;
-      for (int rad = 1; rad <= fp.search_radius && !found; ++rad) {
-        for (int dz = -rad; dz <= rad; ++dz)
-          for (int dy = -rad; dy <= rad; ++dy)
-            for (int ddx = -rad; ddx <= rad; ++ddx) {
-              if (!(abs(ddx) == rad || abs(dy) == rad || abs(dz) == rad)) continue;
-              const int gx = gx0 + ddx, gy = gy0 + dy, gz = gz0 + dz;
-              size_t ci;
-              if (!cell_at(D, gx, gy, gz, ci) || D.obstacle[ci]) continue;
-              const float ddxp = ((float)gx - 0.5f) * dx - tx;
-              const float ddyp = ((float)gy - 0.5f) * dx - ty;
-              const float ddzp = ((float)gz - 0.5f) * dx - tz;
-              const float dn = ddxp * nx + ddyp * ny + ddzp * nz;
-              if (dn <= 0.0f) continue;
-              const float d2 = ddxp * ddxp + ddyp * ddyp + ddzp * ddzp;
-              if (d2 < best) {
-                best = d2;
-                br = D.rho[ci];
-                bux = D.vel[ci]; buy = D.vel[ci + D.dstride]; buz = D.vel[ci + 2 * D.dstride];
-                bd = dn / dx;
-                found = true;
-              }
-            }
-      }
-    }
+    float br, bux, buy, buz, bd;
+    const bool found = probe_side<1>(D, tx, ty, tz, nx, ny, nz, br, bux, buy, buz, bd);
     float p = 0.f, sx = 0.f, sy = 0.f, sz = 0.f;
     if (found) stress_from_cell(fp, br, bux, buy, buz, nx, ny, nz, fmaxf(bd, 0.5f), p, sx, sy, sz);
     if (D.p_map) {
@@ -171,6 +190,41 @@ __global__ void __launch_bounds__(kForceThreads) k_surface_forces(const __grid_c
     for (int w = 0; w < kForceThreads / 32; ++w) s += red[w][threadIdx.x];
     D.partials[(size_t)blockIdx.x * 9 + threadIdx.x] = s;
   }
+}
+
+// Two-sided net force per triangle in one pass: compute_net_aerodynamics!
+// (surface.jl:980-1034) runs the plus-side map, the minus-side map (open
+// surfaces only; a closed body's minus maps are zero, surface.jl:987-997) and
+// compute_net_triangle_forces_kernel! (surface.jl:665-700) as three launches
+// over the triangles; here one thread does all three for its triangle, so the
+// maps go to memory only when the caller asks for them.
+__global__ void __launch_bounds__(kForceThreads)
+    k_surface_net_forces(const __grid_constant__ ForceDev D,
+                         const __grid_constant__ ol_net_force_maps M, int closed_body) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= D.mesh.n_triangles) return;
+  const ol_force_params &fp = D.fp;
+  const float tx = D.mesh.cx[i] + fp.offset_x, ty = D.mesh.cy[i] + fp.offset_y,
+              tz = D.mesh.cz[i] + fp.offset_z;
+  const float nx = D.mesh.nx[i], ny = D.mesh.ny[i], nz = D.mesh.nz[i];
+  float br, bux, buy, buz, bd;
+  float p = 0.f, sx = 0.f, sy = 0.f, sz = 0.f;
+  if (probe_side<1>(D, tx, ty, tz, nx, ny, nz, br, bux, buy, buz, bd))
+    stress_from_cell(fp, br, bux, buy, buz, nx, ny, nz, fmaxf(bd, 0.5f), p, sx, sy, sz);
+  float pm = 0.f, sxm = 0.f, sym = 0.f, szm = 0.f;
+  if (!closed_body && probe_side<-1>(D, tx, ty, tz, nx, ny, nz, br, bux, buy, buz, bd))
+    stress_from_cell(fp, br, bux, buy, buz, -nx, -ny, -nz, fmaxf(bd, 0.5f), pm, sxm, sym, szm);
+  if (M.p_plus) {
+    M.p_plus[i] = p; M.sx_plus[i] = sx; M.sy_plus[i] = sy; M.sz_plus[i] = sz;
+  }
+  if (M.p_minus) {
+    M.p_minus[i] = pm; M.sx_minus[i] = sxm; M.sy_minus[i] = sym; M.sz_minus[i] = szm;
+  }
+  const float pn = p - pm, snx = sx - sxm, sny = sy - sym, snz = sz - szm;
+  const float A = D.mesh.area[i];
+  M.net_fx[i] = -pn * nx * A + snx * A;
+  M.net_fy[i] = -pn * ny * A + sny * A;
+  M.net_fz[i] = -pn * nz * A + snz * A;
 }
 
 // Fixed-order sum of nvals-wide partial rows: out[j] = sum_b partials[b*nvals + j].
@@ -291,6 +345,35 @@ extern "C" int ol_surface_forces(const ol_surface_mesh *mesh, const float *rho, 
   OL_LAUNCHED("ol_surface_forces");
   OL_CUDA(cudaMemcpyAsync(out, dev_out, 9 * sizeof(double), cudaMemcpyDeviceToHost, s));
   OL_CUDA(cudaStreamSynchronize(s));
+  return OL_OK;
+}
+
+extern "C" int ol_surface_net_forces(const ol_surface_mesh *mesh, const float *rho,
+                                     const float *vel, const uint8_t *obstacle,
+                                     const int32_t *block_ptr, int32_t n_blocks,
+                                     const ol_force_params *fp, int32_t closed_body,
+                                     const ol_net_force_maps *out, void *stream) {
+  OL_CHECK_ARG(mesh && fp && out, "ol_surface_net_forces: null argument");
+  OL_CHECK_ARG(mesh->n_triangles >= 0 && n_blocks > 0, "ol_surface_net_forces: bad sizes");
+  if (mesh->n_triangles == 0) return OL_OK;
+  OL_CHECK_ARG(mesh->cx && mesh->cy && mesh->cz && mesh->nx && mesh->ny && mesh->nz &&
+                   mesh->area && rho && vel && obstacle && block_ptr && out->net_fx &&
+                   out->net_fy && out->net_fz,
+               "ol_surface_net_forces: null device pointer");
+  OL_CHECK_ARG(!out->p_plus == !out->sx_plus && !out->p_plus == !out->sy_plus &&
+                   !out->p_plus == !out->sz_plus && !out->p_minus == !out->sx_minus &&
+                   !out->p_minus == !out->sy_minus && !out->p_minus == !out->sz_minus,
+               "ol_surface_net_forces: each side's maps must be all given or all null");
+  ForceDev D = {};
+  D.mesh = *mesh;
+  D.rho = rho; D.vel = vel; D.obstacle = obstacle; D.bptr = block_ptr;
+  D.block_offset = 0;
+  D.dstride = (int64_t)BCELLS * n_blocks;
+  D.fp = *fp;
+  const int grid = (mesh->n_triangles + kForceThreads - 1) / kForceThreads;
+  k_surface_net_forces<<<grid, kForceThreads, 0, (cudaStream_t)stream>>>(D, *out,
+                                                                          closed_body ? 1 : 0);
+  OL_LAUNCHED("ol_surface_net_forces");
   return OL_OK;
 }
 

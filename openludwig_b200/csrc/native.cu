@@ -119,6 +119,17 @@ __global__ void __launch_bounds__(kGhostThreads, kGhostMinBlocks)
   ghost_fill_block<ST>(L, w.block, ghost_row_of(L, w.block));
 }
 
+// The same for the thermal populations of DDF cases (thermal descriptors).
+template <class ST>
+__global__ void __launch_bounds__(kGhostThreads, kGhostMinBlocks)
+    k_ghost_fill_tb(const ThermalDev *__restrict__ tdescs, const WorkItem *__restrict__ items) {
+  __shared__ __align__(16) ThermalDev D;
+  const WorkItem w = items[blockIdx.x];
+  copy_desc(&D, tdescs + w.desc, threadIdx.x);
+  __syncthreads();
+  ghost_fill_block<ST>(D, w.block, ghost_row_of(D, w.block));
+}
+
 template <int OP, class ST, bool WALE, bool DDF>
 __global__ void __launch_bounds__(512, OP == OL_OP_CUMULANT ? 2 : 1)
     k_sc_batched(const LevelDev *__restrict__ descs, const ThermalDev *__restrict__ tdescs,
@@ -244,6 +255,7 @@ struct DevLevel {
   // refined levels: precomputed absent-neighbour values of the blocks that
   // have an absent neighbour (compact rows), block -> row index
   float *ghost = nullptr;
+  float *ghost_g = nullptr;  // the same rows for the thermal populations (DDF cases)
   int32_t *gidx = nullptr;
   std::vector<int32_t> ghost_blocks;  // host copy of the blocks with a row
 };
@@ -281,7 +293,7 @@ struct NCase {
 };
 
 struct Launch {
-  int kind;     // 0 = stream-collide, 1 = bouzidi gather, 2 = bouzidi scatter, 3 = ghost fill
+  int kind;     // 0 = stream-collide, 1/2 = bouzidi gather/scatter, 3/4 = flow/thermal ghosts
   int op = 0, wale = 0, ddf = 0;
   int64_t off = 0, n = 0;   // items (kind 0) or links (kind 1/2)
 };
@@ -341,7 +353,8 @@ static size_t case_meta_bytes(const ol_case_desc *cd) {
     b += (size_t)L.n_blocks * (27 + 3) * 4 + (size_t)L.dim_x * L.dim_y * L.dim_z * 4;
     b += (size_t)L.n_boundary * (27 * 2 + 4 + 3);
     if (l > 0)
-      b += blocks_with_absent_neighbour(L).size() * kHaloEntries * sizeof(float) +
+      b += blocks_with_absent_neighbour(L).size() * kHaloEntries * sizeof(float) *
+               (cd->ddf ? 2 : 1) +
            (size_t)L.n_blocks * sizeof(int32_t);
   }
   b += (size_t)cd->n_triangles * 7 * 4 + force_partial_rows(cd->n_triangles) * 9 * 8 + 256;
@@ -389,7 +402,7 @@ static void free_case_meta(NCase &c) {
   for (auto &L : c.levels) {
     cudaFree(L.nbr); cudaFree(L.mx); cudaFree(L.my); cudaFree(L.mz); cudaFree(L.bptr);
     cudaFree(L.q); cudaFree(L.cb); cudaFree(L.cx); cudaFree(L.cy); cudaFree(L.cz);
-    cudaFree(L.ghost); cudaFree(L.gidx);
+    cudaFree(L.ghost); cudaFree(L.ghost_g); cudaFree(L.gidx);
   }
   cudaFree(c.mesh);
   cudaFree(c.partials);
@@ -444,6 +457,13 @@ static void record_step(ol_ctx *c) {
     if (l.kind == 0) {
       if (c->f16) launch_sc_dispatch<StoreF16S>(c, l);
       else launch_sc_dispatch<StoreF32>(c, l);
+    } else if (l.kind == 4) {
+      if (c->f16)
+        k_ghost_fill_tb<StoreF16S><<<(unsigned)l.n, kGhostThreads, 0, c->stream>>>(
+            c->d_tdescs, c->d_items + l.off);
+      else
+        k_ghost_fill_tb<StoreF32><<<(unsigned)l.n, kGhostThreads, 0, c->stream>>>(
+            c->d_tdescs, c->d_items + l.off);
     } else if (l.kind == 3) {
       if (c->f16)
         k_ghost_fill_b<StoreF16S><<<(unsigned)l.n, kGhostThreads, 0, c->stream>>>(
@@ -500,7 +520,7 @@ static int rebuild(ol_ctx *c) {
     std::map<int, std::vector<int>> groups;  // variant -> descriptor ids
     int64_t scratch_off = 0;
     std::vector<int> bz_flow, bz_therm;
-    std::vector<WorkItem> ghost_items;
+    std::vector<WorkItem> ghost_items, tghost_items;
     for (auto &kv : c->cases) {
       NCase &cs = *kv.second;
       if ((int)cs.levels.size() < l) continue;
@@ -555,6 +575,9 @@ static int rebuild(ol_ctx *c) {
           D.pptr = PV.bptr; D.pdim_x = PV.dims[0]; D.pdim_y = PV.dims[1]; D.pdim_z = PV.dims[2];
           D.p_block_offset = PV.block_offset; D.p_dstride = dstride;
           D.p_inv_scale = 1.0f / PV.scale;
+          D.ghost = V.ghost_g;
+          D.gidx = V.gidx;
+          for (int32_t b : V.ghost_blocks) tghost_items.push_back(WorkItem{d, b});
         } else {
           D.tp.tau_g_parent = 0.5f;
           D.p_inv_scale = 1.0f;
@@ -592,6 +615,15 @@ static int rebuild(ol_ctx *c) {
       gl.off = (int64_t)items.size();
       items.insert(items.end(), ghost_items.begin(), ghost_items.end());
       gl.n = (int64_t)ghost_items.size();
+      c->plan.push_back(gl);
+      ++per_step;
+    }
+    if (!tghost_items.empty()) {  // and of the thermal populations of DDF cases
+      Launch gl{};
+      gl.kind = 4;
+      gl.off = (int64_t)items.size();
+      items.insert(items.end(), tghost_items.begin(), tghost_items.end());
+      gl.n = (int64_t)tghost_items.size();
       c->plan.push_back(gl);
       ++per_step;
     }
@@ -819,8 +851,11 @@ extern "C" int ol_ctx_case_add(ol_ctx *c, const ol_case_desc *cd, int32_t *case_
       std::vector<int32_t> gi((size_t)S.n_blocks, -1);
       for (size_t r = 0; r < V.ghost_blocks.size(); ++r) gi[V.ghost_blocks[r]] = (int32_t)r;
       if ((rc = upload(&V.gidx, gi.data(), gi.size()))) return rc;
-      if (!V.ghost_blocks.empty())
+      if (!V.ghost_blocks.empty()) {
         OL_CUDA(cudaMalloc(&V.ghost, V.ghost_blocks.size() * kHaloEntries * sizeof(float)));
+        if (cd->ddf)
+          OL_CUDA(cudaMalloc(&V.ghost_g, V.ghost_blocks.size() * kHaloEntries * sizeof(float)));
+      }
     }
     V.n_boundary = S.n_boundary;
     if (S.n_boundary > 0) {
@@ -1027,6 +1062,46 @@ extern "C" int ol_ctx_case_download(ol_ctx *c, int32_t id, int32_t level, float 
     cudaStreamSynchronize(c->stream);
     cudaFree(tmp);
     if (e != cudaSuccess) return cuda_status(e, "ol_ctx_case_download");
+  }
+  return OL_OK;
+}
+
+extern "C" int ol_ctx_case_download_thermal(ol_ctx *c, int32_t id, int32_t level, float *T,
+                                            float *g) {
+  OL_CHECK_ARG(c, "ol_ctx_case_download_thermal: null context");
+  std::lock_guard<std::mutex> lk(c->mu);
+  auto it = c->cases.find(id);
+  if (it == c->cases.end())
+    return set_error(OL_ERR_STATE, "ol_ctx_case_download_thermal: unknown case %d", id);
+  NCase &cs = *it->second;
+  OL_CHECK_ARG(cs.ddf, "ol_ctx_case_download_thermal: case %d has no thermal DDF", id);
+  OL_CHECK_ARG(level >= 1 && level <= (int)cs.levels.size(),
+               "ol_ctx_case_download_thermal: bad level");
+  const DevLevel &V = cs.levels[level - 1];
+  // the last sub-step of the level wrote the same half of each A/B pair as rho and f
+  const int64_t t = cs.steps;
+  const int lv = level - 1;
+  const int64_t last = t * ((int64_t)1 << lv) + (((int64_t)1 << lv) - 1);
+  const bool even = (last & 1) == 0;
+  float *dT = t == 0 ? c->P.TA : (even ? c->P.TB : c->P.TA);
+  void *dg = t == 0 ? c->P.gA : (even ? c->P.gB : c->P.gA);
+  OL_CUDA(cudaStreamSynchronize(c->stream));
+  const size_t c0 = (size_t)V.block_offset * BCELLS, nc = (size_t)V.n_blocks * BCELLS;
+  const size_t dstride = (size_t)c->capacity * BCELLS;
+  if (T) OL_CUDA(cudaMemcpy(T, dT + c0, nc * 4, cudaMemcpyDeviceToHost));
+  if (g) {
+    float *tmp = nullptr;
+    OL_CUDA(cudaMalloc(&tmp, nc * 27 * 4));
+    if (c->f16)
+      k_decode_region<StoreF16S><<<(unsigned)((nc + 255) / 256), 256, 0, c->stream>>>(
+          dg, c0, nc, dstride, 1.0f / V.scale, tmp);
+    else
+      k_decode_region<StoreF32><<<(unsigned)((nc + 255) / 256), 256, 0, c->stream>>>(
+          dg, c0, nc, dstride, 1.0f, tmp);
+    cudaError_t e = cudaMemcpyAsync(g, tmp, nc * 27 * 4, cudaMemcpyDeviceToHost, c->stream);
+    cudaStreamSynchronize(c->stream);
+    cudaFree(tmp);
+    if (e != cudaSuccess) return cuda_status(e, "ol_ctx_case_download_thermal");
   }
   return OL_OK;
 }

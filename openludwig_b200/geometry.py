@@ -258,6 +258,19 @@ def cube(side: float = 1.0, center=(0.0, 0.0, 0.0)) -> SolverMesh:
     return make_mesh(tris)
 
 
+def flat_plate(side: float = 1.0, n: int = 8, center=(0.0, 0.0, 0.0)) -> SolverMesh:
+    """Open square plate of zero thickness in the x-y plane, normal +z,
+    n x n panels of 2 triangles: a thin surface with fluid on both sides."""
+    s = np.linspace(-side / 2.0, side / 2.0, n + 1)
+    tris = []
+    for j in range(n):
+        for i in range(n):
+            a, b = (s[i], s[j], 0.0), (s[i + 1], s[j], 0.0)
+            c, d = (s[i + 1], s[j + 1], 0.0), (s[i], s[j + 1], 0.0)
+            tris.append([a, b, c]); tris.append([a, c, d])
+    return make_mesh(np.array(tris, dtype=np.float64) + np.asarray(center, dtype=np.float64))
+
+
 def naca0012_wing(chord: float = 1.0, span: float = 3.0, n_chord: int = 200, n_span: int = 40,
                   center=(0.0, 0.0, 0.0)) -> SolverMesh:
     """Closed rectangular NACA0012 wing: chord along x, span along y, thickness

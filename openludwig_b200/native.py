@@ -263,6 +263,15 @@ class Context:
         N.call("ol_ctx_case_download", self._h, cid, level, _p(rho), _p(vel), _p(ff))
         return rho, vel, ff
 
+    def download_thermal(self, cid: int, level: int = 1, g: bool = False):
+        """Temperature (and decoded thermal populations) of a DDF case."""
+        h = self.cases[cid].levels[level - 1]
+        n = h.n_blocks * 512
+        T = np.empty(n, np.float32)
+        gg = np.empty(27 * n, np.float32) if g else None
+        N.call("ol_ctx_case_download_thermal", self._h, cid, level, _p(T), _p(gg))
+        return T, gg
+
     def info(self, cid: int) -> tuple[int, int]:
         steps = C.c_int64()
         status = C.c_int32()

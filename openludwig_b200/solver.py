@@ -433,6 +433,27 @@ def compute_aerodynamics(lv: DeviceLevel, dmesh: DeviceMesh, p: DomainParams, cf
     return (raw, m) if maps else raw
 
 
+def compute_net_aerodynamics(lv: DeviceLevel, dmesh: DeviceMesh, p: DomainParams,
+                             cfg: CaseConfig, search_radius: int = 5, closed_body: bool = True,
+                             maps: bool = False):
+    """compute_net_aerodynamics! (surface.jl:980-1034): per-triangle net force
+    (net_Fx, net_Fy, net_Fz) as float32 numpy arrays.  With maps=True also the
+    [8, n] device tensor of plus maps (p, tau x/y/z) and minus maps."""
+    fp = force_params_for(lv, p, cfg, search_radius)
+    n = dmesh.n
+    dev = lv.rho.device
+    net = torch.empty((3, n), dtype=torch.float32, device=dev)
+    m = torch.empty((8, n), dtype=torch.float32, device=dev) if maps else None
+    mp = [_ptr(m[j]) for j in range(8)] if maps else [None] * 8
+    out = N.NetForceMaps(*mp, _ptr(net[0]), _ptr(net[1]), _ptr(net[2]))
+    N.call("ol_surface_net_forces", C.byref(dmesh.view()), _ptr(lv.rho), _ptr(lv.vel),
+           _ptr(lv.obstacle), _ptr(lv.block_ptr), N.i32(lv.n_blocks), C.byref(fp),
+           N.i32(1 if closed_body else 0), C.byref(out), _stream())
+    h = net.cpu().numpy()
+    res = (h[0], h[1], h[2])
+    return (res, m) if maps else res
+
+
 def flow_stats(lv: DeviceLevel) -> dict:
     """compute_flow_stats (diagnostics.jl:43-93) in FP64."""
     partials = torch.empty(int(N.lib().ol_flow_stats_scratch_doubles(lv.n_blocks)),

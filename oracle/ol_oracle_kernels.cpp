@@ -797,6 +797,57 @@ static void stress(const ForceP &fp, float rho, float ux, float uy, float uz, fl
   }
 }
 
+// Flow sample on one side of a triangle: side +1 follows map_stresses_kernel!
+// (surface.jl:380-483, probes along +n, shell search accepts dot > 0), side -1
+// map_minus_side_only_kernel! (surface.jl:545-640, probes along -n, accepts
+// dot < 0, wall distance |dot| / dx).
+static bool probe_side(int side, const float *rho, const float *vel, const uint8_t *obs,
+                       const int32_t *bptr, size_t S, const ForceP &fp, float tx, float ty,
+                       float tz, float n_x, float n_y, float n_z, float &br, float &bux,
+                       float &buy, float &buz, float &bd) {
+  br = 1.0f; bux = buy = buz = 0.0f; bd = 1.0f;
+  float bq = 0.0f;
+  bool found = false;
+  for (int pi = 1; pi <= fp.search_radius; ++pi) {
+    float dc = (float)pi + 0.5f;
+    float px, py, pz;
+    if (side > 0) {
+      px = tx + n_x * dc * fp.dx; py = ty + n_y * dc * fp.dx; pz = tz + n_z * dc * fp.dx;
+    } else {
+      px = tx - n_x * dc * fp.dx; py = ty - n_y * dc * fp.dx; pz = tz - n_z * dc * fp.dx;
+    }
+    float r, ux, uy, uz, wq;
+    bool ok = trilinear(rho, vel, obs, bptr, S, fp, px, py, pz, r, ux, uy, uz, wq);
+    if (ok && wq >= 0.5f) { br = r; bux = ux; buy = uy; buz = uz; bd = dc; bq = wq; found = true; break; }
+    if (ok && wq > bq) { br = r; bux = ux; buy = uy; buz = uz; bd = dc; bq = wq; found = true; }
+  }
+  if (found) return true;
+  int gx0 = (int)std::floor(tx / fp.dx) + 1, gy0 = (int)std::floor(ty / fp.dx) + 1,
+      gz0 = (int)std::floor(tz / fp.dx) + 1;
+  float best = 1e10f;
+  for (int rad = 1; rad <= fp.search_radius; ++rad) {
+    if (found) break;
+    for (int dz = -rad; dz <= rad; ++dz)
+      for (int dy = -rad; dy <= rad; ++dy)
+        for (int ddx = -rad; ddx <= rad; ++ddx) {
+          if (!(std::abs(ddx) == rad || std::abs(dy) == rad || std::abs(dz) == rad)) continue;
+          int gx = gx0 + ddx, gy = gy0 + dy, gz = gz0 + dz;
+          size_t ci;
+          if (!cell_at(bptr, fp, gx, gy, gz, ci) || obs[ci]) continue;
+          float ddxp = ((float)gx - 0.5f) * fp.dx - tx, ddyp = ((float)gy - 0.5f) * fp.dx - ty,
+                ddzp = ((float)gz - 0.5f) * fp.dx - tz;
+          float dn = ddxp * n_x + ddyp * n_y + ddzp * n_z;
+          if (side > 0 ? dn <= 0.0f : dn >= 0.0f) continue;
+          float d2 = ddxp * ddxp + ddyp * ddyp + ddzp * ddzp;
+          if (d2 < best) {
+            best = d2; br = rho[ci]; bux = vel[ci]; buy = vel[ci + S]; buz = vel[ci + 2 * S];
+            bd = (side > 0 ? dn : std::fabs(dn)) / fp.dx; found = true;
+          }
+        }
+  }
+  return found;
+}
+
 }  // namespace orc
 
 using namespace orc;
@@ -922,41 +973,9 @@ void orc_surface_forces(const float *cx, const float *cy, const float *cz, const
   for (int i = 0; i < ntri; ++i) {
     float tx = cx[i] + fp.off_x, ty = cy[i] + fp.off_y, tz = cz[i] + fp.off_z;
     float n_x = nx[i], n_y = ny[i], n_z = nz[i];
-    float br = 1.0f, bux = 0, buy = 0, buz = 0, bd = 1.0f, bq = 0.0f;
-    bool found = false;
-    for (int pi = 1; pi <= fp.search_radius; ++pi) {
-      float dc = (float)pi + 0.5f;
-      float r, ux, uy, uz, wq;
-      bool ok = trilinear(rho, vel, obs, bptr, S, fp, tx + n_x * dc * fp.dx, ty + n_y * dc * fp.dx,
-                          tz + n_z * dc * fp.dx, r, ux, uy, uz, wq);
-      if (ok && wq >= 0.5f) { br = r; bux = ux; buy = uy; buz = uz; bd = dc; bq = wq; found = true; break; }
-      if (ok && wq > bq) { br = r; bux = ux; buy = uy; buz = uz; bd = dc; bq = wq; found = true; }
-    }
-    if (!found) {
-      int gx0 = (int)std::floor(tx / fp.dx) + 1, gy0 = (int)std::floor(ty / fp.dx) + 1,
-          gz0 = (int)std::floor(tz / fp.dx) + 1;
-      float best = 1e10f;
-      for (int rad = 1; rad <= fp.search_radius; ++rad) {
-        if (found) break;
-        for (int dz = -rad; dz <= rad; ++dz)
-          for (int dy = -rad; dy <= rad; ++dy)
-            for (int ddx = -rad; ddx <= rad; ++ddx) {
-              if (!(std::abs(ddx) == rad || std::abs(dy) == rad || std::abs(dz) == rad)) continue;
-              int gx = gx0 + ddx, gy = gy0 + dy, gz = gz0 + dz;
-              size_t ci;
-              if (!cell_at(bptr, fp, gx, gy, gz, ci) || obs[ci]) continue;
-              float ddxp = ((float)gx - 0.5f) * fp.dx - tx, ddyp = ((float)gy - 0.5f) * fp.dx - ty,
-                    ddzp = ((float)gz - 0.5f) * fp.dx - tz;
-              float dn = ddxp * n_x + ddyp * n_y + ddzp * n_z;
-              if (dn <= 0.0f) continue;
-              float d2 = ddxp * ddxp + ddyp * ddyp + ddzp * ddzp;
-              if (d2 < best) {
-                best = d2; br = rho[ci]; bux = vel[ci]; buy = vel[ci + S]; buz = vel[ci + 2 * S];
-                bd = dn / fp.dx; found = true;
-              }
-            }
-      }
-    }
+    float br, bux, buy, buz, bd;
+    bool found = probe_side(1, rho, vel, obs, bptr, S, fp, tx, ty, tz, n_x, n_y, n_z, br, bux, buy,
+                            buz, bd);
     float p = 0, sx = 0, sy = 0, sz = 0;
     if (found) stress(fp, br, bux, buy, buz, n_x, n_y, n_z, rmax(bd, 0.5f), p, sx, sy, sz);
     if (pmap) { pmap[i] = p; sxm[i] = sx; sym[i] = sy; szm[i] = sz; }
@@ -969,6 +988,41 @@ void orc_surface_forces(const float *cx, const float *cy, const float *cz, const
     out[6] += (double)(ry * Fz - rz * Fy);
     out[7] += (double)(rz * Fx - rx * Fz);
     out[8] += (double)(rx * Fy - ry * Fx);
+  }
+}
+
+// Two-sided per-triangle net force, compute_net_aerodynamics! (surface.jl:980-1034):
+// plus-side stresses as map_stresses_kernel!; minus side zero for a closed body
+// (surface.jl:987-997), else map_minus_side_only_kernel! (surface.jl:511-662,
+// stress evaluated with the normal -n); then compute_net_triangle_forces_kernel!
+// (surface.jl:665-700): F = -(p+ - p-) n A + (tau+ - tau-) A.
+// maps: [8][ntri] = p+, tau+ x/y/z, p-, tau- x/y/z; net: [3][ntri].
+void orc_surface_net_forces(const float *cx, const float *cy, const float *cz, const float *nx,
+                            const float *ny, const float *nz, const float *area, int32_t ntri,
+                            const float *rho, const float *vel, const uint8_t *obs,
+                            const int32_t *bptr, int32_t nB, const ForceP *fpp,
+                            int32_t closed_body, float *maps, float *net) {
+  const ForceP &fp = *fpp;
+  const size_t S = (size_t)NC * nB;
+  const size_t T = (size_t)ntri;
+  for (int i = 0; i < ntri; ++i) {
+    float tx = cx[i] + fp.off_x, ty = cy[i] + fp.off_y, tz = cz[i] + fp.off_z;
+    float n_x = nx[i], n_y = ny[i], n_z = nz[i];
+    float br, bux, buy, buz, bd;
+    float p = 0, sx = 0, sy = 0, sz = 0;
+    if (probe_side(1, rho, vel, obs, bptr, S, fp, tx, ty, tz, n_x, n_y, n_z, br, bux, buy, buz, bd))
+      stress(fp, br, bux, buy, buz, n_x, n_y, n_z, rmax(bd, 0.5f), p, sx, sy, sz);
+    float pm = 0, sxm = 0, sym = 0, szm = 0;
+    if (!closed_body &&
+        probe_side(-1, rho, vel, obs, bptr, S, fp, tx, ty, tz, n_x, n_y, n_z, br, bux, buy, buz, bd))
+      stress(fp, br, bux, buy, buz, -n_x, -n_y, -n_z, rmax(bd, 0.5f), pm, sxm, sym, szm);
+    maps[i] = p; maps[T + i] = sx; maps[2 * T + i] = sy; maps[3 * T + i] = sz;
+    maps[4 * T + i] = pm; maps[5 * T + i] = sxm; maps[6 * T + i] = sym; maps[7 * T + i] = szm;
+    float pn = p - pm, snx = sx - sxm, sny = sy - sym, snz = sz - szm;
+    float A = area[i];
+    net[i] = -pn * n_x * A + snx * A;
+    net[T + i] = -pn * n_y * A + sny * A;
+    net[2 * T + i] = -pn * n_z * A + snz * A;
   }
 }
 

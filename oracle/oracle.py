@@ -216,6 +216,22 @@ def surface_forces(mesh_arrays, rho, vel, obstacle, block_ptr, n_blocks, fp_stru
     return out, maps
 
 
+def surface_net_forces(mesh_arrays, rho, vel, obstacle, block_ptr, n_blocks, fp_struct,
+                       closed_body: bool):
+    """Two-sided per-triangle net forces: returns maps [8, n] (p+, tau+ xyz,
+    p-, tau- xyz) and net [3, n] (Fx, Fy, Fz)."""
+    m = np.ascontiguousarray(mesh_arrays, dtype=np.float32)
+    n = m.shape[1]
+    maps = np.zeros((8, n), np.float32)
+    net = np.zeros((3, n), np.float32)
+    fp = ForceParamsC()
+    C.memmove(C.byref(fp), C.byref(fp_struct), C.sizeof(fp))
+    lib().orc_surface_net_forces(*[_p(m[i]) for i in range(7)], C.c_int32(n), _p(rho), _p(vel),
+                                 _p(obstacle), _p(block_ptr), C.c_int32(n_blocks), C.byref(fp),
+                                 C.c_int32(1 if closed_body else 0), _p(maps), _p(net))
+    return maps, net
+
+
 def double_to_half_bits(x: float) -> int:
     fn = lib().orc_double_to_half
     fn.restype = C.c_uint16

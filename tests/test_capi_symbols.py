@@ -69,7 +69,8 @@ def test_ctypes_struct_layouts_match_header(tmp_path):
              "ol_step_params": N.StepParams, "ol_thermal_params": N.ThermalParams,
              "ol_force_params": N.ForceParams, "ol_level_view": N.LevelView,
              "ol_parent_view": N.ParentView, "ol_thermal_view": N.ThermalView,
-             "ol_surface_mesh": N.SurfaceMesh, "ol_restrict_view": N.RestrictView}
+             "ol_surface_mesh": N.SurfaceMesh, "ol_restrict_view": N.RestrictView,
+             "ol_net_force_maps": N.NetForceMaps}
     src = tmp_path / "sizes.c"
     src.write_text('#include <stdio.h>\n#include "openludwig_b200.h"\nint main(void){\n' +
                    "".join(f'printf("%zu\\n", sizeof({n}));\n' for n in names) + "return 0;}\n")

@@ -47,15 +47,25 @@ def test_fp32_and_fp16_against_fp64_oracle():
                                   o.vel.astype(np.float32), lv.obstacle.cpu().numpy(),
                                   lv.block_ptr.cpu().numpy(), lv.n_blocks, fp)
     ref = (p.rho_physical, p.u_physical, p.reference_area, p.reference_chord)
-    cd64 = NT.coefficients(raw64, *ref).Cd
-    cd32 = NT.coefficients(raw32, *ref).Cd
+    c64, c32 = NT.coefficients(raw64, *ref), NT.coefficients(raw32, *ref)
+    cd64, cd32 = c64.Cd, c32.Cd
     assert cd64 > 0.0
     assert abs(cd32 - cd64) <= 5e-3 * abs(cd64)
+    # mass drift: total density against the FP64 run's
+    m32, m64 = float(lv.rho.double().sum()), float(o.rho.sum())
+    assert abs(m32 - m64) <= 1e-6 * m64
 
     case = NT.PreparedCase(c, mesh, p, hosts, sim.settings)
     ctx = NT.Context(budget_bytes=1 << 30, storage="f16")
     cid = ctx.add_case(case)
     ctx.step(STEPS)
-    cd16 = ctx.forces(cid).Cd
+    c16 = ctx.forces(cid)
+    rho16 = ctx.download(cid, 1)[0]
     ctx.close()
-    assert abs(cd16 - cd64) <= 1e-2 * abs(cd64)
+    assert abs(c16.Cd - cd64) <= 1e-2 * abs(cd64)
+    m16 = float(np.asarray(rho16, np.float64).sum())
+    print(f"\naccuracy vs FP64 after {STEPS} steps: FP32 rho L2 {rel_err(lv.rho.cpu().numpy(), o.rho):.2e}"
+          f" u L2 {rel_err(lv.vel.cpu().numpy(), o.vel):.2e} Cd {abs(cd32 / cd64 - 1):.2e}"
+          f" Cl {abs(c32.Cl - c64.Cl):.2e} (abs) mass {abs(m32 / m64 - 1):.2e};"
+          f" FP16 storage Cd {abs(c16.Cd / cd64 - 1):.2e} Cl {abs(c16.Cl - c64.Cl):.2e} (abs)"
+          f" mass {abs(m16 / m64 - 1):.2e}")

@@ -73,6 +73,31 @@ def test_native_f32_matches_dropin(which, request):
     ctx.close()
 
 
+def test_native_ddf_matches_dropin():
+    """Thermal DDF in the pool (refined-level ghost rows for f and g filled in
+    the coarse-step graph) against the drop-in path, both FP32."""
+    case = _case(16, 2, c_wale=np.float32(0.5), compressibility_correction=True,
+                 ddf_enabled=True, u_target=np.float32(0.1))
+    steps = 6
+    ctx = NT.Context(budget_bytes=2 << 30, storage="f32", ddf=True)
+    cid = ctx.add_case(case)
+    ctx.step(steps)
+    ctx.sync()
+    levels = [S.upload_level(h, DEV, ddf=True) for h in case.levels]
+    dims = (case.params.nx_coarse, case.params.ny_coarse, case.params.nz_coarse)
+    for t in range(1, steps + 1):
+        S.recursive_step(levels, case.settings, 0, t, None, 0.0, float(case.cfg.u_target), dims)
+    torch.cuda.synchronize()
+    for lvl, lv in enumerate(levels, start=1):
+        sub = 1 << (lvl - 1)
+        last = steps * sub + sub - 1
+        newest_g = lv.g_temp if last % 2 == 0 else lv.g
+        T, g = ctx.download_thermal(cid, lvl, g=True)
+        assert rel_err(g, newest_g.cpu().numpy()) < 1e-6
+        assert rel_err(T, lv.temperature.cpu().numpy()) < 1e-6
+    ctx.close()
+
+
 def test_alone_equals_in_mix(one_level, two_level):
     steps = 8
     a = NT.Context(budget_bytes=2 << 30, storage="f16")

@@ -7,7 +7,10 @@ the method and from exact integer / IEEE arithmetic:
   * binary16 rounding of q against numpy's IEEE conversion,
   * collision invariants: mass and momentum conservation of the cumulant and
     regularized-BGK collisions, rest state as a fixed point,
-  * Bouzidi at q = 1/2 equals half-way bounce-back and at q = 1 the average.
+  * Bouzidi at q = 1/2 equals half-way bounce-back and at q = 1 the average,
+  * restriction keeps equilibrium, mass and momentum,
+  * two-sided net force on an open plate at rest vanishes; closed-body mode
+    leaves -p n A.
 """
 import numpy as np
 import pytest
@@ -175,3 +178,36 @@ def test_restriction_keeps_equilibrium_and_conserves_mass_momentum():
         assert got.sum() == pytest.approx(mean.sum(), rel=1e-12)
         assert (got * cx).sum() == pytest.approx((mean * cx).sum(), abs=1e-12)
         assert (got * cz).sum() == pytest.approx((mean * cz).sum(), abs=1e-12)
+
+
+def test_net_forces_of_a_plate_at_rest():
+    """Two-sided net force (surface.jl:511-700) on an open plate in fluid at
+    rest with uniform density: both sides see the same pressure (up to the
+    rounding of the fluid-weighted trilinear average) and no shear, so the
+    open-surface net force vanishes per triangle, while the closed-body mode
+    (minus side zero) leaves the one-sided -p n A."""
+    import types
+    from openludwig_b200 import domain, geometry as geo, scaling, solver as S, workloads
+    c, _ = workloads.sphere_1lvl(8)
+    c.alpha_deg = 15.0
+    mesh = geo.rotate_mesh(geo.flat_plate(1.0, 8), 15.0, 0.0)
+    p = scaling.compute_domain_from_mesh(c, mesh.min_bounds, mesh.max_bounds)
+    h = domain.setup_multilevel_domain(c, mesh, p)[-1]
+    fp = S.force_params_for(types.SimpleNamespace(host=h), p, c)
+    a = np.stack([mesh.centers[:, 0], mesh.centers[:, 1], mesh.centers[:, 2], mesh.normals[:, 0],
+                  mesh.normals[:, 1], mesh.normals[:, 2], mesh.areas]).astype(np.float32)
+    rho = np.full(512 * h.n_blocks, 1.02, np.float32)
+    vel = np.zeros(3 * 512 * h.n_blocks, np.float32)
+    maps, net = orc.surface_net_forces(a, rho, vel, h.obstacle, h.block_ptr, h.n_blocks, fp,
+                                       False)
+    p0 = np.float32((np.float32(1.02) - np.float32(1)) / np.float32(3)) * np.float32(fp.pressure_scale)
+    # every triangle found fluid on both sides
+    np.testing.assert_allclose(maps[0], p0, rtol=5e-5)
+    np.testing.assert_allclose(maps[4], p0, rtol=5e-5)
+    assert not maps[1:4].any() and not maps[5:8].any()
+    assert np.abs(net).max() <= 5e-5 * p0 * a[6].max()
+    maps, net = orc.surface_net_forces(a, rho, vel, h.obstacle, h.block_ptr, h.n_blocks, fp,
+                                       True)
+    assert not maps[4:].any()
+    expect = -p0 * a[3:6] * a[6]
+    np.testing.assert_allclose(net, expect, rtol=5e-5, atol=5e-5 * p0 * a[6].max())
