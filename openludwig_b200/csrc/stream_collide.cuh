@@ -69,18 +69,34 @@ __device__ __forceinline__ float trilerp(const float (&v)[8], float wx, float wy
   return lerp_rn(c0, c1, wz);
 }
 
+// Temporal blend of a parent value: lerp_rn(old, new, tw), or new alone
+// without temporal interpolation.  At tw = 0 (the first child sub-step of a
+// parent step) (1 - 0) * old + 0 * new rounds to old for every finite new, so
+// `new` is not read there: half the parent gathers of that sub-step.
+template <class NEW>
+__device__ __forceinline__ float blend_parent(bool temporal, float tw, float old_v, NEW new_v) {
+  if (!temporal) return new_v();
+  if (tw == 0.0f) return old_v;
+  return lerp_rn(old_v, new_v(), tw);
+}
+
 // Blended parent moments (rho, ux, uy, uz) of the present parent cell c.
 __device__ __forceinline__ void corner_moments(const LevelDev &L, int64_t c, float (&m)[4]) {
   const ol_step_params &sp = L.sp;
   const bool temporal = sp.use_temporal_interp == 1 && sp.temporal_weight < 0.99f;
   const float tw = sp.temporal_weight;
-  const float rn = L.prho[c], uxn = L.pvel[c], uyn = L.pvel[c + L.p_dstride],
-              uzn = L.pvel[c + 2 * L.p_dstride];
+  const int64_t S = L.p_dstride;
+  if (temporal && tw == 0.0f) {
+    m[0] = L.prho_old[c]; m[1] = L.pvel_old[c];
+    m[2] = L.pvel_old[c + S]; m[3] = L.pvel_old[c + 2 * S];
+    return;
+  }
+  const float rn = L.prho[c], uxn = L.pvel[c], uyn = L.pvel[c + S], uzn = L.pvel[c + 2 * S];
   if (temporal) {
     m[0] = lerp_rn(L.prho_old[c], rn, tw);
     m[1] = lerp_rn(L.pvel_old[c], uxn, tw);
-    m[2] = lerp_rn(L.pvel_old[c + L.p_dstride], uyn, tw);
-    m[3] = lerp_rn(L.pvel_old[c + 2 * L.p_dstride], uzn, tw);
+    m[2] = lerp_rn(L.pvel_old[c + S], uyn, tw);
+    m[3] = lerp_rn(L.pvel_old[c + 2 * S], uzn, tw);
   } else {
     m[0] = rn; m[1] = uxn; m[2] = uyn; m[3] = uzn;
   }
@@ -92,10 +108,10 @@ __device__ __forceinline__ float corner_population(const LevelDev &L, int64_t c,
   const ol_step_params &sp = L.sp;
   const bool temporal = sp.use_temporal_interp == 1 && sp.temporal_weight < 0.99f;
   const size_t a = (size_t)c + (size_t)k * L.p_dstride;
-  const float fn = ST::load((const typename ST::T *)L.pf, a, k, L.p_inv_scale);
-  return temporal ? lerp_rn(ST::load((const typename ST::T *)L.pf_old, a, k, L.p_inv_scale), fn,
-                            sp.temporal_weight)
-                  : fn;
+  using T = typename ST::T;
+  const float fo = temporal ? ST::load((const T *)L.pf_old, a, k, L.p_inv_scale) : 0.0f;
+  return blend_parent(temporal, sp.temporal_weight, fo,
+                      [&] { return ST::load((const T *)L.pf, a, k, L.p_inv_scale); });
 }
 
 // Parent rho, ux, uy, uz at the ghost position: each corner blended between

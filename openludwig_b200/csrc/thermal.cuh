@@ -42,7 +42,10 @@ __device__ __forceinline__ void ghost_moments(const ThermalDev &D, const ParentS
   for (int s = 0; s < 8; ++s) {
     v[0][s] = 1.0f; v[1][s] = 0.0f; v[2][s] = 0.0f; v[3][s] = 0.0f;
     const int64_t c = P.ci[s];
-    if (c >= 0) {
+    if (c >= 0 && temporal && tw == 0.0f) {   // old state alone (blend_parent)
+      v[0][s] = D.pT_old[c]; v[1][s] = D.pvel_old[c];
+      v[2][s] = D.pvel_old[c + D.p_dstride]; v[3][s] = D.pvel_old[c + 2 * D.p_dstride];
+    } else if (c >= 0) {
       const float Tn = D.pT[c], uxn = D.pvel[c], uyn = D.pvel[c + D.p_dstride],
                   uzn = D.pvel[c + 2 * D.p_dstride];
       if (temporal) {
@@ -77,10 +80,10 @@ __device__ __forceinline__ float ghost_population(const ThermalDev &D, int k,
     const int64_t c = P.ci[s];
     if (c >= 0) {
       const size_t a = (size_t)c + (size_t)k * D.p_dstride;
-      const float gn = ST::load((const typename ST::T *)D.pg, a, k, D.p_inv_scale);
-      v[s] = temporal ? lerp_rn(ST::load((const typename ST::T *)D.pg_old, a, k, D.p_inv_scale),
-                                gn, tp.temporal_weight)
-                      : gn;
+      using T = typename ST::T;
+      const float go = temporal ? ST::load((const T *)D.pg_old, a, k, D.p_inv_scale) : 0.0f;
+      v[s] = blend_parent(temporal, tp.temporal_weight, go,
+                          [&] { return ST::load((const T *)D.pg, a, k, D.p_inv_scale); });
     }
   }
 #pragma unroll
