@@ -74,7 +74,29 @@ typedef struct ol_level_view {
   const int32_t *map_x, *map_y, *map_z; /* [nB] 1-based block coordinates     */
   float *ghost;                 /* [ol_ghost_floats(nB)] scratch, or NULL (below) */
   int32_t n_blocks;
+  /* Optional pairing of the two sub-steps a fine level takes per parent step
+   * (temporal weights 0 and 1/2, solver_control.jl:65-97), with ghost set:
+   * OL_GHOST_PAIR_FIRST on the weight-0 call also writes into ghost_next (a
+   * second [ol_ghost_floats(nB)] scratch) the coarse-to-fine values of the
+   * weight-1/2 call, reading each parent value once for both;
+   * OL_GHOST_PAIR_SECOND on the weight-1/2 call, with ghost = that
+   * ghost_next and the parent state unchanged since, evaluates only the
+   * domain-boundary values.  OL_GHOST_UNPAIRED (0) computes every value in
+   * every call.  Results are identical in all three modes. */
+  float *ghost_next;
+  int32_t ghost_mode;
+  /* Optional [n_ghost_blocks] 0-based ids of the blocks the ghost pass visits
+   * (NULL = every block; the pass skips blocks without an absent neighbour).
+   * A list must hold every block with an absent neighbour, or under
+   * OL_GHOST_PAIR_SECOND every block with an absent neighbour not wholly
+   * inside the level's domain; it saves the launch of the other blocks. */
+  const int32_t *ghost_blocks;
+  int32_t n_ghost_blocks;
 } ol_level_view;
+
+#define OL_GHOST_UNPAIRED 0
+#define OL_GHOST_PAIR_FIRST 1
+#define OL_GHOST_PAIR_SECOND 2
 
 /* Size (floats) of the optional ol_level_view.ghost scratch.  No reference
  * counterpart: with ghost set, ol_stream_collide first evaluates, in a
@@ -174,6 +196,10 @@ typedef struct ol_thermal_view {
   /* optional [ol_ghost_floats(nB)] scratch, as ol_level_view.ghost: the
    * boundary values of absent neighbours by a separate pass (same results) */
   float *ghost;
+  float *ghost_next;             /* as ol_level_view.ghost_next / ghost_mode */
+  int32_t ghost_mode;
+  const int32_t *ghost_blocks;   /* as ol_level_view.ghost_blocks            */
+  int32_t n_ghost_blocks;
 } ol_thermal_view;
 
 typedef struct ol_thermal_params {

@@ -15,6 +15,7 @@ OL_OP_CUMULANT = 0
 OL_OP_REGULARIZED_BGK = 1
 OL_LIMITER_NONE, OL_LIMITER_FACTORED, OL_LIMITER_POSITIVITY = 0, 1, 2
 OL_STORE_F32, OL_STORE_F16, OL_STORE_DDF = 0, 1, 2
+OL_GHOST_UNPAIRED, OL_GHOST_PAIR_FIRST, OL_GHOST_PAIR_SECOND = 0, 1, 2
 
 vp = C.c_void_p
 i32 = C.c_int32
@@ -25,7 +26,8 @@ class LevelView(C.Structure):
     _fields_ = [("f_out", vp), ("f_in", vp), ("f_post", vp), ("rho", vp), ("vel_out", vp),
                 ("vel_in", vp), ("obstacle", vp), ("sponge", vp), ("wall_dist", vp),
                 ("neighbor_table", vp), ("map_x", vp), ("map_y", vp), ("map_z", vp),
-                ("ghost", vp), ("n_blocks", i32)]
+                ("ghost", vp), ("n_blocks", i32), ("ghost_next", vp), ("ghost_mode", i32),
+                ("ghost_blocks", vp), ("n_ghost_blocks", i32)]
 
 
 class ParentView(C.Structure):
@@ -55,7 +57,8 @@ class ThermalView(C.Structure):
                 ("map_y", vp), ("map_z", vp), ("n_blocks", i32),
                 ("pg", vp), ("pT", vp), ("pvel", vp), ("pg_old", vp), ("pT_old", vp),
                 ("pvel_old", vp), ("p_block_ptr", vp), ("p_dim_x", i32), ("p_dim_y", i32),
-                ("p_dim_z", i32), ("p_n_blocks", i32), ("ghost", vp)]
+                ("p_dim_z", i32), ("p_n_blocks", i32), ("ghost", vp), ("ghost_next", vp),
+                ("ghost_mode", i32), ("ghost_blocks", vp), ("n_ghost_blocks", i32)]
 
 
 THERMAL_FIELDS = [("tau_g", f32), ("tau_g_parent", f32), ("is_level_1", i32),

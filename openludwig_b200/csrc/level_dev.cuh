@@ -69,7 +69,19 @@ struct LevelDev {
   const uint32_t *halo_tab;  // staging table (stream_collide.cuh)
   float *ghost;           // absent-neighbour pull sources, kHaloEntries per row, or null
   const int32_t *gidx;    // block -> ghost row (-1: none); null = row b for block b
+  // Pairing of the two child sub-steps of one parent step (kGhost* below):
+  // 1 = this first sub-step also writes the second one's coarse-to-fine
+  // values into ghost_next (same row layout); 2 = ghost already holds them
+  // and only the domain-boundary slots are evaluated; 0 = no pairing.
+  float *ghost_next;
+  int32_t ghost_mode;
+  const int32_t *gblocks;  // blocks the drop-in ghost pass visits (null = all)
+  int32_t n_gblocks;
 };
+
+constexpr int kGhostUnpaired = 0, kGhostPairFirst = 1, kGhostPairSecond = 2;
+// temporal weight of the second child sub-step (solver_control.jl:65-97)
+constexpr float kSecondSubstepWeight = 0.5f;
 
 // One unit of batched work: block `block` of the level described by
 // descriptor `desc`.

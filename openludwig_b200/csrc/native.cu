@@ -116,7 +116,7 @@ __global__ void __launch_bounds__(kGhostThreads, kGhostMinBlocks)
   const WorkItem w = items[blockIdx.x];
   copy_desc(&L, descs + w.desc, threadIdx.x);
   __syncthreads();
-  ghost_fill_block<ST>(L, w.block, ghost_row_of(L, w.block));
+  ghost_fill_block<ST>(L, w.block, ghost_row_of(L, w.block), ghost_next_row_of(L, w.block));
 }
 
 // The same for the thermal populations of DDF cases (thermal descriptors).
@@ -127,7 +127,7 @@ __global__ void __launch_bounds__(kGhostThreads, kGhostMinBlocks)
   const WorkItem w = items[blockIdx.x];
   copy_desc(&D, tdescs + w.desc, threadIdx.x);
   __syncthreads();
-  ghost_fill_block<ST>(D, w.block, ghost_row_of(D, w.block));
+  ghost_fill_block<ST>(D, w.block, ghost_row_of(D, w.block), ghost_next_row_of(D, w.block));
 }
 
 template <int OP, class ST, bool WALE, bool DDF>
@@ -256,8 +256,13 @@ struct DevLevel {
   // have an absent neighbour (compact rows), block -> row index
   float *ghost = nullptr;
   float *ghost_g = nullptr;  // the same rows for the thermal populations (DDF cases)
+  // rows of the second child sub-step of each parent step, written by the
+  // first one's ghost pass (ghost pairing, LevelDev::ghost_mode)
+  float *ghost2 = nullptr;
+  float *ghost_g2 = nullptr;
   int32_t *gidx = nullptr;
   std::vector<int32_t> ghost_blocks;  // host copy of the blocks with a row
+  std::vector<int32_t> edge_blocks;   // those of them with domain-boundary values
 };
 
 // Blocks of a level with at least one absent neighbour (neighbour table
@@ -270,6 +275,28 @@ static std::vector<int32_t> blocks_with_absent_neighbour(const ol_level_desc &S)
         out.push_back(b);
         break;
       }
+  return out;
+}
+
+// Of `ghost`, the blocks with an absent neighbour not wholly inside the
+// level's domain (n*_global cells per axis): the only blocks whose values
+// the second sub-step of a pair evaluates (domain boundary conditions); every
+// other absent-neighbour value is coarse-to-fine and set by the first.
+static std::vector<int32_t> blocks_with_domain_edge(const ol_level_desc &S,
+                                                    const std::vector<int32_t> &ghost, int nxg,
+                                                    int nyg, int nzg) {
+  std::vector<int32_t> out;
+  auto inside = [](int nb, int ng) { return nb >= 1 && (int64_t)nb * BS <= ng; };
+  for (int32_t b : ghost)
+    for (int d = 0; d < 27; ++d) {
+      if (S.neighbor_table[b + (size_t)S.n_blocks * d] > 0) continue;
+      const int nbx = S.map_x[b] + d % 3 - 1, nby = S.map_y[b] + (d / 3) % 3 - 1,
+                nbz = S.map_z[b] + d / 9 - 1;
+      if (!inside(nbx, nxg) || !inside(nby, nyg) || !inside(nbz, nzg)) {
+        out.push_back(b);
+        break;
+      }
+    }
   return out;
 }
 
@@ -352,8 +379,8 @@ static size_t case_meta_bytes(const ol_case_desc *cd) {
     const ol_level_desc &L = cd->levels[l];
     b += (size_t)L.n_blocks * (27 + 3) * 4 + (size_t)L.dim_x * L.dim_y * L.dim_z * 4;
     b += (size_t)L.n_boundary * (27 * 2 + 4 + 3);
-    if (l > 0)
-      b += blocks_with_absent_neighbour(L).size() * kHaloEntries * sizeof(float) *
+    if (l > 0)  // ghost rows of both sub-steps of a pair, flow (+ thermal)
+      b += blocks_with_absent_neighbour(L).size() * kHaloEntries * sizeof(float) * 2 *
                (cd->ddf ? 2 : 1) +
            (size_t)L.n_blocks * sizeof(int32_t);
   }
@@ -402,7 +429,8 @@ static void free_case_meta(NCase &c) {
   for (auto &L : c.levels) {
     cudaFree(L.nbr); cudaFree(L.mx); cudaFree(L.my); cudaFree(L.mz); cudaFree(L.bptr);
     cudaFree(L.q); cudaFree(L.cb); cudaFree(L.cx); cudaFree(L.cy); cudaFree(L.cz);
-    cudaFree(L.ghost); cudaFree(L.ghost_g); cudaFree(L.gidx);
+    cudaFree(L.ghost); cudaFree(L.ghost_g); cudaFree(L.ghost2); cudaFree(L.ghost_g2);
+    cudaFree(L.gidx);
   }
   cudaFree(c.mesh);
   cudaFree(c.partials);
@@ -550,9 +578,15 @@ static int rebuild(ol_ctx *c) {
         L.p_block_offset = PV.block_offset;
         L.p_dstride = dstride;
         L.p_inv_scale = 1.0f / PV.scale;
-        L.ghost = V.ghost;
+        // j even: first child sub-step of a parent step (weight 0), j odd:
+        // the second (weight 1/2); for level >= 2 the parity of t_sub is j's
+        const bool first = (j & 1) == 0;
+        L.ghost = first ? V.ghost : V.ghost2;
+        L.ghost_next = V.ghost2;
+        L.ghost_mode = first ? kGhostPairFirst : kGhostPairSecond;
         L.gidx = V.gidx;
-        for (int32_t b : V.ghost_blocks) ghost_items.push_back(WorkItem{d, b});
+        for (int32_t b : first ? V.ghost_blocks : V.edge_blocks)
+          ghost_items.push_back(WorkItem{d, b});
       } else {
         L.sp.tau_parent = 0.5f;
         L.p_inv_scale = 1.0f;
@@ -575,9 +609,13 @@ static int rebuild(ol_ctx *c) {
           D.pptr = PV.bptr; D.pdim_x = PV.dims[0]; D.pdim_y = PV.dims[1]; D.pdim_z = PV.dims[2];
           D.p_block_offset = PV.block_offset; D.p_dstride = dstride;
           D.p_inv_scale = 1.0f / PV.scale;
-          D.ghost = V.ghost_g;
+          const bool first = (j & 1) == 0;
+          D.ghost = first ? V.ghost_g : V.ghost_g2;
+          D.ghost_next = V.ghost_g2;
+          D.ghost_mode = first ? kGhostPairFirst : kGhostPairSecond;
           D.gidx = V.gidx;
-          for (int32_t b : V.ghost_blocks) tghost_items.push_back(WorkItem{d, b});
+          for (int32_t b : first ? V.ghost_blocks : V.edge_blocks)
+            tghost_items.push_back(WorkItem{d, b});
         } else {
           D.tp.tau_g_parent = 0.5f;
           D.p_inv_scale = 1.0f;
@@ -851,10 +889,17 @@ extern "C" int ol_ctx_case_add(ol_ctx *c, const ol_case_desc *cd, int32_t *case_
       std::vector<int32_t> gi((size_t)S.n_blocks, -1);
       for (size_t r = 0; r < V.ghost_blocks.size(); ++r) gi[V.ghost_blocks[r]] = (int32_t)r;
       if ((rc = upload(&V.gidx, gi.data(), gi.size()))) return rc;
+      const int sc = 1 << l;
+      V.edge_blocks = blocks_with_domain_edge(S, V.ghost_blocks, cd->nx * sc, cd->ny * sc,
+                                              cd->nz * sc);
       if (!V.ghost_blocks.empty()) {
-        OL_CUDA(cudaMalloc(&V.ghost, V.ghost_blocks.size() * kHaloEntries * sizeof(float)));
-        if (cd->ddf)
-          OL_CUDA(cudaMalloc(&V.ghost_g, V.ghost_blocks.size() * kHaloEntries * sizeof(float)));
+        const size_t gb = V.ghost_blocks.size() * kHaloEntries * sizeof(float);
+        OL_CUDA(cudaMalloc(&V.ghost, gb));
+        OL_CUDA(cudaMalloc(&V.ghost2, gb));
+        if (cd->ddf) {
+          OL_CUDA(cudaMalloc(&V.ghost_g, gb));
+          OL_CUDA(cudaMalloc(&V.ghost_g2, gb));
+        }
       }
     }
     V.n_boundary = S.n_boundary;

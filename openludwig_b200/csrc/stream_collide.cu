@@ -134,9 +134,10 @@ static bool use_pipeline() {
 
 void launch_stream_collide(const LevelDev &L, bool f16, cudaStream_t s) {
   if (L.n_blocks <= 0) return;
-  if (L.ghost) {
-    if (f16) k_ghost_fill<StoreF16S><<<L.n_blocks, kGhostThreads, 0, s>>>(L);
-    else k_ghost_fill<StoreF32><<<L.n_blocks, kGhostThreads, 0, s>>>(L);
+  const int gn = L.gblocks ? L.n_gblocks : L.n_blocks;
+  if (L.ghost && gn > 0) {
+    if (f16) k_ghost_fill<StoreF16S><<<gn, kGhostThreads, 0, s>>>(L);
+    else k_ghost_fill<StoreF32><<<gn, kGhostThreads, 0, s>>>(L);
   }
   if (f16 || !use_pipeline()) {
     if (!f16) { launch_sc<StoreF32>(L, s); return; }
@@ -202,6 +203,23 @@ extern "C" int ol_stream_collide(const ol_level_view *lv, const ol_parent_view *
   L.nbr_stride = lv->n_blocks;
   L.scale = 1.0f; L.inv_scale = 1.0f; L.p_inv_scale = 1.0f;
   L.ghost = lv->ghost;
+  L.ghost_next = lv->ghost_next;
+  L.ghost_mode = lv->ghost_mode;
+  L.gblocks = lv->ghost_blocks;
+  L.n_gblocks = lv->n_ghost_blocks;
+  OL_CHECK_ARG(lv->n_ghost_blocks >= 0 && lv->n_ghost_blocks <= lv->n_blocks &&
+                   (lv->n_ghost_blocks == 0 || lv->ghost_blocks),
+               "ol_stream_collide: bad ghost block list");
+  OL_CHECK_ARG(lv->ghost_mode >= OL_GHOST_UNPAIRED && lv->ghost_mode <= OL_GHOST_PAIR_SECOND,
+               "ol_stream_collide: unknown ghost_mode %d", lv->ghost_mode);
+  OL_CHECK_ARG(lv->ghost_mode == OL_GHOST_UNPAIRED || (lv->ghost && !sp->is_level_1),
+               "ol_stream_collide: ghost pairing needs a fine level and the ghost scratch");
+  OL_CHECK_ARG(lv->ghost_mode != OL_GHOST_PAIR_FIRST ||
+                   (lv->ghost_next && lv->ghost_next != lv->ghost && sp->temporal_weight == 0.0f),
+               "ol_stream_collide: OL_GHOST_PAIR_FIRST needs a distinct ghost_next and "
+               "temporal weight 0");
+  OL_CHECK_ARG(lv->ghost_mode != OL_GHOST_PAIR_SECOND || sp->temporal_weight == 0.5f,
+               "ol_stream_collide: OL_GHOST_PAIR_SECOND needs temporal weight 1/2");
   L.sp = *sp;
   OL_CHECK_ARG((int64_t)lv->n_blocks * BCELLS < (1LL << 31),
                "ol_stream_collide: n_blocks too large for 32-bit plane offsets");

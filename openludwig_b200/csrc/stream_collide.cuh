@@ -80,11 +80,11 @@ __device__ __forceinline__ float blend_parent(bool temporal, float tw, float old
   return lerp_rn(old_v, new_v(), tw);
 }
 
-// Blended parent moments (rho, ux, uy, uz) of the present parent cell c.
-__device__ __forceinline__ void corner_moments(const LevelDev &L, int64_t c, float (&m)[4]) {
-  const ol_step_params &sp = L.sp;
-  const bool temporal = sp.use_temporal_interp == 1 && sp.temporal_weight < 0.99f;
-  const float tw = sp.temporal_weight;
+// Blended parent moments (rho, ux, uy, uz) of the present parent cell c at
+// temporal weight tw.
+__device__ __forceinline__ void corner_moments(const LevelDev &L, int64_t c, float tw,
+                                               float (&m)[4]) {
+  const bool temporal = L.sp.use_temporal_interp == 1 && tw < 0.99f;
   const int64_t S = L.p_dstride;
   if (temporal && tw == 0.0f) {
     m[0] = L.prho_old[c]; m[1] = L.pvel_old[c];
@@ -102,15 +102,15 @@ __device__ __forceinline__ void corner_moments(const LevelDev &L, int64_t c, flo
   }
 }
 
-// Blended parent population k of the present parent cell c.
+// Blended parent population k of the present parent cell c at weight tw.
 template <class ST>
-__device__ __forceinline__ float corner_population(const LevelDev &L, int64_t c, int k) {
-  const ol_step_params &sp = L.sp;
-  const bool temporal = sp.use_temporal_interp == 1 && sp.temporal_weight < 0.99f;
+__device__ __forceinline__ float corner_population(const LevelDev &L, int64_t c, int k,
+                                                   float tw) {
+  const bool temporal = L.sp.use_temporal_interp == 1 && tw < 0.99f;
   const size_t a = (size_t)c + (size_t)k * L.p_dstride;
   using T = typename ST::T;
   const float fo = temporal ? ST::load((const T *)L.pf_old, a, k, L.p_inv_scale) : 0.0f;
-  return blend_parent(temporal, sp.temporal_weight, fo,
+  return blend_parent(temporal, tw, fo,
                       [&] { return ST::load((const T *)L.pf, a, k, L.p_inv_scale); });
 }
 
@@ -118,12 +118,12 @@ __device__ __forceinline__ float corner_population(const LevelDev &L, int64_t c,
 // the parent's old and new state, missing corners replaced by the (possibly
 // missing, then rho = 1, u = 0) first corner, then trilinear.
 __device__ __forceinline__ void interp_moments(const LevelDev &L, const ParentStencil &P,
-                                               float (&r)[4]) {
+                                               float tw, float (&r)[4]) {
   float v[4][8];
 #pragma unroll
   for (int s = 0; s < 8; ++s) {
     float m[4] = {1.0f, 0.0f, 0.0f, 0.0f};
-    if (P.ci[s] >= 0) corner_moments(L, P.ci[s], m);
+    if (P.ci[s] >= 0) corner_moments(L, P.ci[s], tw, m);
 #pragma unroll
     for (int i = 0; i < 4; ++i) v[i][s] = m[i];
   }
@@ -153,17 +153,50 @@ __device__ __forceinline__ float finish_population(const LevelDev &L, int k, con
   return __fadd_rn(fe, __fmul_rn(fneq, sc));
 }
 
-// Ghost population k at a position with stencil P and moments r.
+// Ghost population k at a position with stencil P and moments r (weight tw).
 template <class ST>
 __device__ __forceinline__ float interp_population(const LevelDev &L, int k,
-                                                   const ParentStencil &P, const float (&r)[4]) {
+                                                   const ParentStencil &P, const float (&r)[4],
+                                                   float tw) {
   float v[8];
 #pragma unroll
-  for (int s = 0; s < 8; ++s) v[s] = P.ci[s] >= 0 ? corner_population<ST>(L, P.ci[s], k) : w_of(k);
+  for (int s = 0; s < 8; ++s)
+    v[s] = P.ci[s] >= 0 ? corner_population<ST>(L, P.ci[s], k, tw) : w_of(k);
 #pragma unroll
   for (int s = 1; s < 8; ++s)
     if (P.ci[s] < 0) v[s] = v[0];
   return finish_population(L, k, v, P.wx, P.wy, P.wz, r);
+}
+
+// The same population for both child sub-steps of a parent step from one
+// read of the parent's old and new state: g0 at weight 0 (the old state),
+// g1 at kSecondSubstepWeight; r0 / r1 are the moments at those weights.
+// Bitwise what interp_population gives at each weight.
+template <class ST>
+__device__ __forceinline__ void interp_population_pair(const LevelDev &L, int k,
+                                                       const ParentStencil &P,
+                                                       const float (&r0)[4],
+                                                       const float (&r1)[4], float &g0,
+                                                       float &g1) {
+  const bool temporal = L.sp.use_temporal_interp == 1;
+  using T = typename ST::T;
+  float v0[8], v1[8];
+#pragma unroll
+  for (int s = 0; s < 8; ++s) {
+    v0[s] = v1[s] = w_of(k);
+    if (P.ci[s] >= 0) {
+      const size_t a = (size_t)P.ci[s] + (size_t)k * L.p_dstride;
+      const float fn = ST::load((const T *)L.pf, a, k, L.p_inv_scale);
+      const float fo = temporal ? ST::load((const T *)L.pf_old, a, k, L.p_inv_scale) : fn;
+      v0[s] = fo;
+      v1[s] = temporal ? lerp_rn(fo, fn, kSecondSubstepWeight) : fn;
+    }
+  }
+#pragma unroll
+  for (int s = 1; s < 8; ++s)
+    if (P.ci[s] < 0) { v0[s] = v0[0]; v1[s] = v1[0]; }
+  g0 = finish_population(L, k, v0, P.wx, P.wy, P.wz, r0);
+  g1 = finish_population(L, k, v1, P.wx, P.wy, P.wz, r1);
 }
 
 // ---------------------------------------------------------------------------
@@ -539,7 +572,7 @@ __device__ __noinline__ void fill_missing_flow(const LevelDev &L, const int *nbb
         ParentStencil P;
         parent_stencil(L, sgx, sgy, sgz, P);
         float r[4];
-        interp_moments(L, P, r);
+        interp_moments(L, P, sp.temporal_weight, r);
 #pragma unroll
         for (int i = 0; i < 4; ++i) E[stash_plane(ox, oy, oz, i) * EPL + p] = r[i];
       }
@@ -563,7 +596,7 @@ __device__ __noinline__ void fill_missing_flow(const LevelDev &L, const int *nbb
       for (int j = 0; j < 4; ++j) r[j] = E[stash_plane(ox, oy, oz, j) * EPL + p];
       ParentStencil P;
       parent_stencil(L, sgx, sgy, sgz, P);
-      v = interp_population<ST>(L, k, P, r);
+      v = interp_population<ST>(L, k, P, r, sp.temporal_weight);
     } else {
       v = pull_boundary<ST>(L, k, b, sx + cx_of(k), sy + cy_of(k), sz + cz_of(k));
     }
@@ -605,18 +638,32 @@ __device__ __forceinline__ float *ghost_row_of(const DEV &L, int b) {
   const int r = L.gidx ? L.gidx[b] : b;
   return r >= 0 ? L.ghost + (size_t)r * kHaloEntries : nullptr;
 }
+// The same row of ghost_next (written by the first sub-step of a pair).
+template <class DEV>
+__device__ __forceinline__ float *ghost_next_row_of(const DEV &L, int b) {
+  if (L.ghost_mode != kGhostPairFirst || !L.ghost_next) return nullptr;
+  const int r = L.gidx ? L.gidx[b] : b;
+  return r >= 0 ? L.ghost_next + (size_t)r * kHaloEntries : nullptr;
+}
 
 // What the ghost pass needs to know of a flow level; the thermal DDF
-// provides the same four functions for its populations (thermal.cuh).
+// provides the same functions for its populations (thermal.cuh).
 __device__ __forceinline__ const ol_step_params &ghost_params(const LevelDev &L) { return L.sp; }
-__device__ __forceinline__ void ghost_moments(const LevelDev &L, const ParentStencil &P,
+__device__ __forceinline__ void ghost_moments(const LevelDev &L, const ParentStencil &P, float tw,
                                               float (&r)[4]) {
-  interp_moments(L, P, r);
+  interp_moments(L, P, tw, r);
 }
 template <class ST>
 __device__ __forceinline__ float ghost_population(const LevelDev &L, int k, const ParentStencil &P,
-                                                  const float (&r)[4], ST) {
-  return interp_population<ST>(L, k, P, r);
+                                                  const float (&r)[4], float tw, ST) {
+  return interp_population<ST>(L, k, P, r, tw);
+}
+template <class ST>
+__device__ __forceinline__ void ghost_population_pair(const LevelDev &L, int k,
+                                                      const ParentStencil &P,
+                                                      const float (&r0)[4], const float (&r1)[4],
+                                                      ST, float &g0, float &g1) {
+  interp_population_pair<ST>(L, k, P, r0, r1, g0, g1);
 }
 template <class ST>
 __device__ __forceinline__ float ghost_boundary(const LevelDev &L, int k, int b, int x, int y,
@@ -624,31 +671,47 @@ __device__ __forceinline__ float ghost_boundary(const LevelDev &L, int k, int b,
   return pull_boundary<ST>(L, k, b, x, y, z);
 }
 
-// One CTA of kGhostThreads threads evaluates block b's row G.
+// One CTA of kGhostThreads threads evaluates block b's row G.  With
+// L.ghost_mode == kGhostPairFirst it also writes into G2 the coarse-to-fine
+// slots of the pair's second sub-step (the parent does not step in between),
+// reading each parent value once for both; with kGhostPairSecond those slots
+// of G are already set and only the domain-boundary slots are evaluated.
 template <class ST, class DEV>
-__device__ __forceinline__ void ghost_fill_block(const DEV &L, int b, float *G) {
+__device__ __forceinline__ void ghost_fill_block(const DEV &L, int b, float *G, float *G2) {
   __shared__ int nbbase[27];
   __shared__ int n_pos, n_slot;
   __shared__ float rs[4][kRingEntries];     // interpolated rho, ux, uy, uz
+  __shared__ float rs2[4][kRingEntries];    // the same at the second sub-step's weight
   __shared__ int32_t cs[8][kRingEntries];   // parent stencil cells
   __shared__ float ws[3][kRingEntries];     // trilinear weights
   __shared__ int16_t ring_of[EPL];          // staging slot -> ring index
   __shared__ int16_t pos_list[kRingEntries];
   __shared__ int16_t slot_list[kHaloEntries];
   const int t = threadIdx.x;
+  const auto &sp = ghost_params(L);
+  const bool precomputed = L.ghost_mode == kGhostPairSecond;
+  const int mx = L.map_x[b], my = L.map_y[b], mz = L.map_z[b];
   int missing = 0;
   if (t < 27) {
     const int nb = L.nbr[b + L.nbr_stride * t];
     nbbase[t] = nb > 0 ? (int)((L.block_offset + nb - 1) * BCELLS) : -1;
     missing = nb <= 0;
+    if (missing && precomputed) {
+      // the second sub-step of a pair only revisits absent neighbours that are
+      // not wholly inside the domain (all others are coarse-to-fine, set)
+      const int nbx = mx + t % 3 - 1, nby = my + (t / 3) % 3 - 1, nbz = mz + t / 9 - 1;
+      missing = !(nbx >= 1 && nbx * BS <= sp.nx_global && nby >= 1 &&
+                  nby * BS <= sp.ny_global && nbz >= 1 && nbz * BS <= sp.nz_global);
+    }
   }
   if (t == 0) { n_pos = 0; n_slot = 0; }
   if (!__syncthreads_or(missing)) return;
-  const auto &sp = ghost_params(L);
   const uint32_t *__restrict__ tab = L.halo_tab;
   const bool fine = sp.is_level_1 == 0;
-  const int gx0 = (L.map_x[b] - 1) * BS + 1, gy0 = (L.map_y[b] - 1) * BS + 1,
-            gz0 = (L.map_z[b] - 1) * BS + 1;
+  const bool pair = G2 != nullptr;                         // first sub-step of a pair
+  const bool interp = fine && !precomputed;                // this pass interpolates
+  const float tw = sp.temporal_weight;
+  const int gx0 = (mx - 1) * BS + 1, gy0 = (my - 1) * BS + 1, gz0 = (mz - 1) * BS + 1;
   auto in_domain = [&](int gx, int gy, int gz) {
     return gx >= 1 && gx <= sp.nx_global && gy >= 1 && gy <= sp.ny_global && gz >= 1 &&
            gz <= sp.nz_global;
@@ -660,7 +723,7 @@ __device__ __forceinline__ void ghost_fill_block(const DEV &L, int b, float *G) 
     const int i = t + j * kGhostThreads;
     te[j] = i < kHaloEntries ? __ldg(tab + i) : 0u;
   }
-  if (fine) {
+  if (interp) {
     for (int j = 0; j < (kRingEntries + kGhostThreads - 1) / kGhostThreads; ++j) {
       const int q = t + j * kGhostThreads;
       bool want = false;
@@ -683,7 +746,7 @@ __device__ __forceinline__ void ghost_fill_block(const DEV &L, int b, float *G) 
     append_if(i < kHaloEntries && nbbase[(te[j] >> 5) & 31] < 0, i, &n_slot, slot_list);
   }
   __syncthreads();
-  if (fine) {
+  if (interp) {
     for (int j = t; j < n_pos; j += kGhostThreads) {
       const int q = pos_list[j];
       const int p = (int)__ldg(tab + kHaloEntries + q);
@@ -691,9 +754,14 @@ __device__ __forceinline__ void ghost_fill_block(const DEV &L, int b, float *G) 
       ParentStencil P;
       parent_stencil(L, gx0 + sx, gy0 + sy, gz0 + sz, P);
       float r[4];
-      ghost_moments(L, P, r);
+      ghost_moments(L, P, tw, r);
 #pragma unroll
       for (int i = 0; i < 4; ++i) rs[i][q] = r[i];
+      if (pair) {
+        ghost_moments(L, P, kSecondSubstepWeight, r);
+#pragma unroll
+        for (int i = 0; i < 4; ++i) rs2[i][q] = r[i];
+      }
 #pragma unroll
       for (int s = 0; s < 8; ++s) cs[s][q] = (int32_t)P.ci[s];
       ws[0][q] = P.wx; ws[1][q] = P.wy; ws[2][q] = P.wz;
@@ -705,19 +773,26 @@ __device__ __forceinline__ void ghost_fill_block(const DEV &L, int b, float *G) 
     const uint32_t e = __ldg(tab + i);
     const int k = e & 31, p = e >> 19;
     const int sx = p % 10 - 1, sy = (p / 10) % 10 - 1, sz = p / 100 - 1;
-    float v;
     if (fine && in_domain(gx0 + sx, gy0 + sy, gz0 + sz)) {
+      if (precomputed) continue;
       const int q = ring_of[p];
       ParentStencil P;
 #pragma unroll
       for (int s = 0; s < 8; ++s) P.ci[s] = cs[s][q];
       P.wx = ws[0][q]; P.wy = ws[1][q]; P.wz = ws[2][q];
       const float r[4] = {rs[0][q], rs[1][q], rs[2][q], rs[3][q]};
-      v = ghost_population(L, k, P, r, ST{});
+      if (pair) {
+        const float r2[4] = {rs2[0][q], rs2[1][q], rs2[2][q], rs2[3][q]};
+        float g0, g1;
+        ghost_population_pair(L, k, P, r, r2, ST{}, g0, g1);
+        G[i] = g0;
+        G2[i] = g1;
+      } else {
+        G[i] = ghost_population(L, k, P, r, tw, ST{});
+      }
     } else {
-      v = ghost_boundary(L, k, b, sx + cx_of(k), sy + cy_of(k), sz + cz_of(k), ST{});
+      G[i] = ghost_boundary(L, k, b, sx + cx_of(k), sy + cy_of(k), sz + cz_of(k), ST{});
     }
-    G[i] = v;
   }
 }
 
@@ -725,7 +800,8 @@ __device__ __forceinline__ void ghost_fill_block(const DEV &L, int b, float *G) 
 template <class ST>
 __global__ void __launch_bounds__(kGhostThreads, kGhostMinBlocks)
     k_ghost_fill(const __grid_constant__ LevelDev L) {
-  ghost_fill_block<ST>(L, blockIdx.x, L.ghost + (size_t)blockIdx.x * kHaloEntries);
+  const int b = L.gblocks ? L.gblocks[blockIdx.x] : (int)blockIdx.x;
+  ghost_fill_block<ST>(L, b, ghost_row_of(L, b), ghost_next_row_of(L, b));
 }
 
 constexpr int kHaloPerThread = (kHaloEntries + BCELLS - 1) / BCELLS;  // 7

@@ -20,7 +20,8 @@ __global__ void __launch_bounds__(512, 2) k_thermal(const __grid_constant__ Ther
 template <class ST>
 __global__ void __launch_bounds__(kGhostThreads, kGhostMinBlocks)
     k_ghost_fill_thermal(const __grid_constant__ ThermalDev D) {
-  ghost_fill_block<ST>(D, blockIdx.x, D.ghost + (size_t)blockIdx.x * kHaloEntries);
+  const int b = D.gblocks ? D.gblocks[blockIdx.x] : (int)blockIdx.x;
+  ghost_fill_block<ST>(D, b, ghost_row_of(D, b), ghost_next_row_of(D, b));
 }
 
 template <class ST>
@@ -30,7 +31,8 @@ static void launch_t(const ThermalDev &D, cudaStream_t s) {
     cudaFuncSetAttribute(k_thermal<ST>, cudaFuncAttributeMaxDynamicSharedMemorySize, kStageBytes);
     done = true;
   }
-  if (D.ghost) k_ghost_fill_thermal<ST><<<D.n_blocks, kGhostThreads, 0, s>>>(D);
+  const int gn = D.gblocks ? D.n_gblocks : D.n_blocks;
+  if (D.ghost && gn > 0) k_ghost_fill_thermal<ST><<<gn, kGhostThreads, 0, s>>>(D);
   k_thermal<ST><<<D.n_blocks, BCELLS, kStageBytes, s>>>(D);
 }
 
@@ -64,6 +66,23 @@ extern "C" int ol_thermal(const ol_thermal_view *tv, const ol_thermal_params *tp
   D.nbr_stride = tv->n_blocks;
   D.scale = 1.0f; D.inv_scale = 1.0f; D.p_inv_scale = 1.0f;
   D.ghost = tv->ghost;
+  D.ghost_next = tv->ghost_next;
+  D.ghost_mode = tv->ghost_mode;
+  D.gblocks = tv->ghost_blocks;
+  D.n_gblocks = tv->n_ghost_blocks;
+  OL_CHECK_ARG(tv->n_ghost_blocks >= 0 && tv->n_ghost_blocks <= tv->n_blocks &&
+                   (tv->n_ghost_blocks == 0 || tv->ghost_blocks),
+               "ol_thermal: bad ghost block list");
+  OL_CHECK_ARG(tv->ghost_mode >= OL_GHOST_UNPAIRED && tv->ghost_mode <= OL_GHOST_PAIR_SECOND,
+               "ol_thermal: unknown ghost_mode %d", tv->ghost_mode);
+  OL_CHECK_ARG(tv->ghost_mode == OL_GHOST_UNPAIRED || (tv->ghost && !tp->is_level_1),
+               "ol_thermal: ghost pairing needs a fine level and the ghost scratch");
+  OL_CHECK_ARG(tv->ghost_mode != OL_GHOST_PAIR_FIRST ||
+                   (tv->ghost_next && tv->ghost_next != tv->ghost && tp->temporal_weight == 0.0f),
+               "ol_thermal: OL_GHOST_PAIR_FIRST needs a distinct ghost_next and temporal "
+               "weight 0");
+  OL_CHECK_ARG(tv->ghost_mode != OL_GHOST_PAIR_SECOND || tp->temporal_weight == 0.5f,
+               "ol_thermal: OL_GHOST_PAIR_SECOND needs temporal weight 1/2");
   D.tp = *tp;
   D.halo_tab = halo_table_device();
   if (!D.halo_tab) return set_error(OL_ERR_CUDA, "ol_thermal: staging table allocation failed");

@@ -22,6 +22,10 @@ struct ThermalDev {
   const uint32_t *halo_tab;
   float *ghost;            // absent-neighbour pull sources, kHaloEntries per row, or null
   const int32_t *gidx;     // block -> ghost row (-1: none); null = row b for block b
+  float *ghost_next;       // as LevelDev::ghost_next / ghost_mode
+  int32_t ghost_mode;
+  const int32_t *gblocks;  // as LevelDev::gblocks / n_gblocks
+  int32_t n_gblocks;
 };
 
 // Coarse-to-fine thermal ghost (physics_interpolation.jl:135-247), in the
@@ -33,10 +37,8 @@ __device__ __forceinline__ const ol_thermal_params &ghost_params(const ThermalDe
   return D.tp;
 }
 __device__ __forceinline__ void ghost_moments(const ThermalDev &D, const ParentStencil &P,
-                                              float (&r)[4]) {
-  const ol_thermal_params &tp = D.tp;
-  const bool temporal = tp.use_temporal_interp == 1 && tp.temporal_weight < 0.99f;
-  const float tw = tp.temporal_weight;
+                                              float tw, float (&r)[4]) {
+  const bool temporal = D.tp.use_temporal_interp == 1 && tw < 0.99f;
   float v[4][8];
 #pragma unroll
   for (int s = 0; s < 8; ++s) {
@@ -66,31 +68,13 @@ __device__ __forceinline__ void ghost_moments(const ThermalDev &D, const ParentS
 #pragma unroll
   for (int i = 0; i < 4; ++i) r[i] = trilerp(v[i], P.wx, P.wy, P.wz);
 }
-template <class ST>
-__device__ __forceinline__ float ghost_population(const ThermalDev &D, int k,
-                                                  const ParentStencil &P, const float (&r)[4],
-                                                  ST) {
+
+// g_eq(T, u) + (g - g_eq) * clamp(...) from the 8 corner values of g_k.
+__device__ __forceinline__ float finish_thermal(const ThermalDev &D, int k, const float (&v)[8],
+                                                const ParentStencil &P, const float (&r)[4]) {
   const ol_thermal_params &tp = D.tp;
-  const bool temporal = tp.use_temporal_interp == 1 && tp.temporal_weight < 0.99f;
-  const float w = w_of(k);
-  float v[8];
-#pragma unroll
-  for (int s = 0; s < 8; ++s) {
-    v[s] = w;
-    const int64_t c = P.ci[s];
-    if (c >= 0) {
-      const size_t a = (size_t)c + (size_t)k * D.p_dstride;
-      using T = typename ST::T;
-      const float go = temporal ? ST::load((const T *)D.pg_old, a, k, D.p_inv_scale) : 0.0f;
-      v[s] = blend_parent(temporal, tp.temporal_weight, go,
-                          [&] { return ST::load((const T *)D.pg, a, k, D.p_inv_scale); });
-    }
-  }
-#pragma unroll
-  for (int s = 1; s < 8; ++s)
-    if (P.ci[s] < 0) v[s] = v[0];
   const float gi = trilerp(v, P.wx, P.wy, P.wz);
-  const float ge = geq(r[0], r[1], r[2], r[3], w, (float)cx_of(k), (float)cy_of(k),
+  const float ge = geq(r[0], r[1], r[2], r[3], w_of(k), (float)cx_of(k), (float)cy_of(k),
                        (float)cz_of(k));
   const float gneq = gi - ge;
   const float tc = tp.tau_g_parent - 0.5f, tf = tp.tau_g - 0.5f;
@@ -99,13 +83,66 @@ __device__ __forceinline__ float ghost_population(const ThermalDev &D, int k,
 }
 
 template <class ST>
+__device__ __forceinline__ float ghost_population(const ThermalDev &D, int k,
+                                                  const ParentStencil &P, const float (&r)[4],
+                                                  float tw, ST) {
+  const bool temporal = D.tp.use_temporal_interp == 1 && tw < 0.99f;
+  float v[8];
+#pragma unroll
+  for (int s = 0; s < 8; ++s) {
+    v[s] = w_of(k);
+    const int64_t c = P.ci[s];
+    if (c >= 0) {
+      const size_t a = (size_t)c + (size_t)k * D.p_dstride;
+      using T = typename ST::T;
+      const float go = temporal ? ST::load((const T *)D.pg_old, a, k, D.p_inv_scale) : 0.0f;
+      v[s] = blend_parent(temporal, tw, go,
+                          [&] { return ST::load((const T *)D.pg, a, k, D.p_inv_scale); });
+    }
+  }
+#pragma unroll
+  for (int s = 1; s < 8; ++s)
+    if (P.ci[s] < 0) v[s] = v[0];
+  return finish_thermal(D, k, v, P, r);
+}
+
+// Both child sub-steps of a parent step from one read of the parent's old
+// and new g (as interp_population_pair for the flow).
+template <class ST>
+__device__ __forceinline__ void ghost_population_pair(const ThermalDev &D, int k,
+                                                      const ParentStencil &P,
+                                                      const float (&r0)[4], const float (&r1)[4],
+                                                      ST, float &g0, float &g1) {
+  const bool temporal = D.tp.use_temporal_interp == 1;
+  using T = typename ST::T;
+  float v0[8], v1[8];
+#pragma unroll
+  for (int s = 0; s < 8; ++s) {
+    v0[s] = v1[s] = w_of(k);
+    const int64_t c = P.ci[s];
+    if (c >= 0) {
+      const size_t a = (size_t)c + (size_t)k * D.p_dstride;
+      const float gn = ST::load((const T *)D.pg, a, k, D.p_inv_scale);
+      const float go = temporal ? ST::load((const T *)D.pg_old, a, k, D.p_inv_scale) : gn;
+      v0[s] = go;
+      v1[s] = temporal ? lerp_rn(go, gn, kSecondSubstepWeight) : gn;
+    }
+  }
+#pragma unroll
+  for (int s = 1; s < 8; ++s)
+    if (P.ci[s] < 0) { v0[s] = v0[0]; v1[s] = v1[0]; }
+  g0 = finish_thermal(D, k, v0, P, r0);
+  g1 = finish_thermal(D, k, v1, P, r1);
+}
+
+template <class ST>
 __device__ __noinline__ float interp_parent_thermal(const ThermalDev &D, int k, int gx,
                                                     int gy, int gz) {
   ParentStencil P;
   parent_stencil(D, gx, gy, gz, P);
   float r[4];
-  ghost_moments(D, P, r);
-  return ghost_population(D, k, P, r, ST{});
+  ghost_moments(D, P, D.tp.temporal_weight, r);
+  return ghost_population(D, k, P, r, D.tp.temporal_weight, ST{});
 }
 
 // kernel_thermal.jl:90-130

@@ -70,6 +70,14 @@ class DeviceLevel:
     # absent-neighbour pull sources, precomputed by a separate pass (optional)
     ghost: torch.Tensor | None = None
     ghost_g: torch.Tensor | None = None   # the same for the thermal populations
+    # second scratch of a refined level: the pair's first sub-step writes the
+    # second one's coarse-to-fine values there (ol_level_view.ghost_mode)
+    ghost2: torch.Tensor | None = None
+    ghost_g2: torch.Tensor | None = None
+    # blocks the ghost pass visits: those with an absent neighbour, and those
+    # with one not wholly inside the domain (second sub-step of a pair)
+    ghost_list: torch.Tensor | None = None
+    edge_list: torch.Tensor | None = None
     # thermal DDF
     g: torch.Tensor | None = None
     g_temp: torch.Tensor | None = None
@@ -134,15 +142,36 @@ def upload_level(h: HostLevel, device: torch.device, ddf: bool = False, t_init: 
     if ghost:
         lv.ghost = torch.empty(int(N.lib().ol_ghost_floats(N.i32(n))), dtype=torch.float32,
                                device=dev)
+        if h.level_id > 1:
+            lv.ghost2 = torch.empty_like(lv.ghost)
     if ddf:
         if ghost:
             lv.ghost_g = torch.empty_like(lv.ghost)
+            if h.level_id > 1:
+                lv.ghost_g2 = torch.empty_like(lv.ghost)
         w = torch.tensor(lattice_weights(), dtype=torch.float32, device=dev)
         lv.g = (w[:, None] * t_init).expand(27, S).reshape(-1).clone()
         lv.g_temp = lv.g.clone()
         lv.temperature = torch.full((S,), t_init, dtype=torch.float32, device=dev)
         lv.temperature_old = lv.temperature.clone()
     return lv
+
+
+def ghost_block_lists(h: HostLevel, dims) -> tuple[np.ndarray, np.ndarray]:
+    """0-based ids (int32) of the blocks with an absent neighbour, and of
+    those with an absent neighbour block not wholly inside the level's
+    domain (dims = its size in cells): the ghost pass's visit lists."""
+    n = h.n_blocks
+    missing = np.asarray(h.neighbor_table).reshape(27, n) <= 0     # [dir, block]
+    d = np.arange(27)
+    inside = np.ones((27, n), dtype=bool)
+    for m, off, nc in ((h.map_x, d % 3 - 1, dims[0]), (h.map_y, (d // 3) % 3 - 1, dims[1]),
+                       (h.map_z, d // 9 - 1, dims[2])):
+        c = np.asarray(m, dtype=np.int64)[None, :] + off[:, None]
+        inside &= (c >= 1) & (c * BS <= nc)
+    ghost = np.nonzero(missing.any(axis=0))[0].astype(np.int32)
+    edge = np.nonzero((missing & ~inside).any(axis=0))[0].astype(np.int32)
+    return ghost, edge
 
 
 def lattice_weights() -> list:
@@ -237,10 +266,26 @@ class ParentRef:
     g_new: torch.Tensor | None
 
 
+def _ghost_views(view, lv: DeviceLevel, ghost, ghost2, mode: int) -> None:
+    """Set a view's ghost, ghost_next, ghost_mode and visit list: mode 1 =
+    first sub-step of a pair (also fills ghost2), 2 = second (reads ghost2),
+    0 = unpaired."""
+    if ghost is None or ghost2 is None:
+        mode = N.OL_GHOST_UNPAIRED
+    view.ghost_mode = mode
+    view.ghost = _ptr(ghost2 if mode == N.OL_GHOST_PAIR_SECOND else ghost)
+    view.ghost_next = _ptr(ghost2) if mode == N.OL_GHOST_PAIR_FIRST else None
+    lst = lv.edge_list if mode == N.OL_GHOST_PAIR_SECOND else lv.ghost_list
+    if ghost is not None and lst is not None:
+        view.ghost_blocks, view.n_ghost_blocks = _ptr(lst), int(lst.numel())
+
+
 def perform_timestep(s: StepSettings, lv: DeviceLevel, parent: ParentRef | None, f_out, f_in,
                      vel_out, vel_in, u: float, t_sub: int, tw: float, domain_dims,
-                     g_out=None, g_in=None) -> None:
-    """timestep.jl:1-159: flow kernel, Bouzidi, thermal kernel, thermal Bouzidi."""
+                     g_out=None, g_in=None, ghost_mode: int = 0) -> None:
+    """timestep.jl:1-159: flow kernel, Bouzidi, thermal kernel, thermal Bouzidi.
+    ghost_mode pairs the two sub-steps of a refined level per parent step
+    (N.OL_GHOST_PAIR_FIRST at weight 0, N.OL_GHOST_PAIR_SECOND at 1/2)."""
     n = lv.n_blocks
     if n == 0:
         return
@@ -248,6 +293,10 @@ def perform_timestep(s: StepSettings, lv: DeviceLevel, parent: ParentRef | None,
     scale = 1 << (lv.host.level_id - 1)
     dims = (domain_dims[0] * scale, domain_dims[1] * scale, domain_dims[2] * scale)
     ref_post = lv.f_post is not None
+    if lv.ghost is not None and lv.ghost_list is None:   # static: computed on first use
+        gl, el = ghost_block_lists(lv.host, dims)
+        lv.ghost_list = torch.from_numpy(gl).to(lv.f.device)
+        lv.edge_list = torch.from_numpy(el).to(lv.f.device)
     sp = step_params(s, lv, parent.lv.tau if parent else 0.5, is_l1, dims, u, t_sub, tw,
                      lv.has_bouzidi and ref_post)
     view = N.LevelView(f_out=_ptr(f_out), f_in=_ptr(f_in), f_post=_ptr(lv.f_post),
@@ -255,7 +304,8 @@ def perform_timestep(s: StepSettings, lv: DeviceLevel, parent: ParentRef | None,
                        obstacle=_ptr(lv.obstacle), sponge=_ptr(lv.sponge),
                        wall_dist=_ptr(lv.wall_dist), neighbor_table=_ptr(lv.neighbor_table),
                        map_x=_ptr(lv.map_x), map_y=_ptr(lv.map_y), map_z=_ptr(lv.map_z),
-                       ghost=_ptr(lv.ghost), n_blocks=n)
+                       n_blocks=n)
+    _ghost_views(view, lv, lv.ghost, lv.ghost2, ghost_mode)
     pv = N.ParentView()
     if parent is not None:
         p = parent.lv
@@ -288,8 +338,8 @@ def perform_timestep(s: StepSettings, lv: DeviceLevel, parent: ParentRef | None,
                            temperature=_ptr(lv.temperature), vel=_ptr(vel_out),
                            obstacle=_ptr(lv.obstacle), sponge=_ptr(lv.sponge),
                            neighbor_table=_ptr(lv.neighbor_table), map_x=_ptr(lv.map_x),
-                           map_y=_ptr(lv.map_y), map_z=_ptr(lv.map_z), n_blocks=n,
-                           ghost=_ptr(lv.ghost_g))
+                           map_y=_ptr(lv.map_y), map_z=_ptr(lv.map_z), n_blocks=n)
+        _ghost_views(tv, lv, lv.ghost_g, lv.ghost_g2, ghost_mode)
         if parent is not None:
             p = parent.lv
             d = p.host.grid_dim
@@ -307,8 +357,9 @@ def perform_timestep(s: StepSettings, lv: DeviceLevel, parent: ParentRef | None,
 
 
 def recursive_step(levels: list, s: StepSettings, lvl: int, t_sub: int, parent: ParentRef | None,
-                   tw: float, u: float, domain_dims) -> None:
-    """solver_control.jl:6-197 (recursive_step! and recursive_step_temporal!)."""
+                   tw: float, u: float, domain_dims, ghost_mode: int = 0) -> None:
+    """solver_control.jl:6-197 (recursive_step! and recursive_step_temporal!).
+    A child's two sub-steps per parent step share one ghost pass (ghost_mode)."""
     if lvl >= len(levels):
         return
     lv = levels[lvl]
@@ -328,11 +379,14 @@ def recursive_step(levels: list, s: StepSettings, lvl: int, t_sub: int, parent: 
             lv.temperature_old.copy_(lv.temperature)
     perform_timestep(s, lv, parent, f_out, f_in, vel_out, vel_in, u, t_sub,
                      0.0 if parent is None else tw, domain_dims,
-                     g_out=g_out if s.ddf else None, g_in=g_in if s.ddf else None)
+                     g_out=g_out if s.ddf else None, g_in=g_in if s.ddf else None,
+                     ghost_mode=ghost_mode)
     if has_children:
         me = ParentRef(lv, f_out, vel_out, g_out if s.ddf else None)
-        recursive_step(levels, s, lvl + 1, 2 * t_sub, me, 0.0, u, domain_dims)
-        recursive_step(levels, s, lvl + 1, 2 * t_sub + 1, me, 0.5, u, domain_dims)
+        recursive_step(levels, s, lvl + 1, 2 * t_sub, me, 0.0, u, domain_dims,
+                       N.OL_GHOST_PAIR_FIRST)
+        recursive_step(levels, s, lvl + 1, 2 * t_sub + 1, me, 0.5, u, domain_dims,
+                       N.OL_GHOST_PAIR_SECOND)
         if s.restriction:
             # the child's second sub-step (odd t_sub) wrote f and vel
             restrict_level(levels[lvl + 1], me, s)

@@ -28,6 +28,18 @@ def small_sphere_case(resolution: int = 8, levels: int = 1, bouzidi: bool = True
     return c, mesh, p, hosts
 
 
+def interior_refined_case():
+    """Two-level cube (48 finest cells, Re 1.6e5, alpha 3.2, beta -1.9) whose
+    refined level lies inside the domain: all its absent-neighbour values
+    are coarse-to-fine (4096 fine blocks, 1352 at the interface)."""
+    m = workloads.MixCase("cube", 48, 2, 158378.0, 3.18, -1.94)
+    c, mesh = workloads.mix_case_config(m)
+    c.ramp_steps = 0
+    p = scaling.compute_domain_from_mesh(c, mesh.min_bounds, mesh.max_bounds)
+    hosts = domain.setup_multilevel_domain(c, mesh, p)
+    return c, mesh, p, hosts
+
+
 def lattice():
     cx, cy, cz = [], [], []
     for z in (-1, 0, 1):

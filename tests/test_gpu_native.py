@@ -12,7 +12,7 @@
 import numpy as np
 import pytest
 
-from helpers import rel_err, small_sphere_case
+from helpers import interior_refined_case, rel_err, small_sphere_case
 
 pytestmark = pytest.mark.gpu
 torch = pytest.importorskip("torch")
@@ -52,8 +52,16 @@ def _dropin(case, steps):
     return levels
 
 
-@pytest.mark.parametrize("which", ["one_level", "two_level"])
+@pytest.fixture(scope="module")
+def interior_two_level():
+    c, mesh, p, hosts = interior_refined_case()
+    return NT.PreparedCase(c, mesh, p, hosts, S.StepSettings.from_config(c, c.wall_model_enabled))
+
+
+@pytest.mark.parametrize("which", ["one_level", "two_level", "interior_two_level"])
 def test_native_f32_matches_dropin(which, request):
+    """interior_two_level: no refined block has a domain-boundary value, so
+    the second sub-step of each pair launches no ghost pass at all."""
     case = request.getfixturevalue(which)
     steps = 10
     ctx = NT.Context(budget_bytes=2 << 30, storage="f32")

@@ -12,7 +12,8 @@ import ctypes as C
 import numpy as np
 import pytest
 
-from helpers import max_abs, perturbed_state, rel_err, small_sphere_case, weights32
+from helpers import (interior_refined_case, max_abs, perturbed_state, rel_err,
+                     small_sphere_case, weights32)
 
 pytestmark = pytest.mark.gpu
 
@@ -191,6 +192,40 @@ def test_ghost_pass_equals_inline_fill(ddf):
         assert torch.equal(la.vel_temp, lb.vel_temp) and torch.equal(la.rho, lb.rho)
         if ddf:
             assert la.ghost_g is not None
+            assert torch.equal(la.g_temp, lb.g_temp) and torch.equal(la.g, lb.g)
+            assert torch.equal(la.temperature, lb.temperature)
+
+
+@pytest.mark.parametrize("which", ["interior", "edge_ddf"])
+def test_ghost_pairing_is_bitwise_neutral(which):
+    """The pair's first sub-step filling the second one's coarse-to-fine
+    values (OL_GHOST_PAIR_FIRST / _SECOND) gives the bits of evaluating every
+    value in every call: on a refined level inside the domain (the second
+    pass has nothing left to do) and, with the thermal DDF, on one whose
+    blocks also carry domain-boundary values."""
+    if which == "interior":
+        c, mesh, p, hosts = interior_refined_case()
+        st = S.StepSettings.from_config(c, c.wall_model_enabled)
+        ddf, u, steps = False, 0.05, 4
+    else:
+        c, mesh, p, hosts = small_sphere_case(resolution=16, levels=2, c_wale=np.float32(0.5),
+                                              compressibility_correction=True,
+                                              ddf_enabled=True, u_target=np.float32(0.1))
+        st = S.StepSettings.from_config(c, False)
+        ddf, u, steps = True, 0.1, 6
+    paired = _run_gpu(hosts, p, st, steps, u, ddf=ddf, ghost=True)
+    levels = [S.upload_level(h, DEV, ddf=ddf, ghost=True) for h in hosts]
+    for lv in levels:
+        lv.ghost2 = lv.ghost_g2 = None          # unpaired: every value in every call
+    dims = (p.nx_coarse, p.ny_coarse, p.nz_coarse)
+    for t in range(1, steps + 1):
+        S.recursive_step(levels, st, 0, t, None, 0.0, u, dims)
+    torch.cuda.synchronize()
+    assert paired[1].ghost2 is not None
+    for la, lb in zip(paired, levels):
+        assert torch.equal(la.f_temp, lb.f_temp) and torch.equal(la.f, lb.f)
+        assert torch.equal(la.vel_temp, lb.vel_temp) and torch.equal(la.rho, lb.rho)
+        if ddf:
             assert torch.equal(la.g_temp, lb.g_temp) and torch.equal(la.g, lb.g)
             assert torch.equal(la.temperature, lb.temperature)
 
