@@ -24,33 +24,38 @@ struct ParentStencil {
   float wx, wy, wz;  // trilinear weights
 };
 
+// Trilinear weights of the fine cell (gx, gy, gz) in the parent grid and the
+// parent cell of corner s (bit 0: x + 1, bit 1: y + 1, bit 2: z + 1), or -1
+// when that parent cell does not exist.
 template <class DEV>
-__device__ __forceinline__ void parent_stencil(const DEV &L, int gx, int gy, int gz,
-                                               ParentStencil &P) {
+__device__ __forceinline__ int64_t parent_corner(const DEV &L, int gx, int gy, int gz, int s,
+                                                 float &wx, float &wy, float &wz) {
   const float pxc = ((float)gx - 0.5f) * 0.5f;
   const float pyc = ((float)gy - 0.5f) * 0.5f;
   const float pzc = ((float)gz - 0.5f) * 0.5f;
-  int px0 = (int)floorf(pxc), py0 = (int)floorf(pyc), pz0 = (int)floorf(pzc);
-  const int px1 = px0 + 1, py1 = py0 + 1, pz1 = pz0 + 1;
-  P.wx = pxc - (float)px0;
-  P.wy = pyc - (float)py0;
-  P.wz = pzc - (float)pz0;
-  px0 = max(1, px0); py0 = max(1, py0); pz0 = max(1, pz0);
-#pragma unroll
-  for (int s = 0; s < 8; ++s) {
-    const int pgx = (s & 1) ? px1 : px0;
-    const int pgy = (s & 2) ? py1 : py0;
-    const int pgz = (s & 4) ? pz1 : pz0;
-    const int pbx = (pgx - 1) / BS + 1, pby = (pgy - 1) / BS + 1, pbz = (pgz - 1) / BS + 1;
-    P.ci[s] = -1;
-    if (pbx >= 1 && pbx <= L.pdim_x && pby >= 1 && pby <= L.pdim_y && pbz >= 1 &&
-        pbz <= L.pdim_z) {
-      const int pb = L.pptr[(pbx - 1) + L.pdim_x * ((pby - 1) + L.pdim_y * (pbz - 1))];
-      if (pb > 0)
-        P.ci[s] = (int64_t)(L.p_block_offset + pb - 1) * BCELLS + (pgx - 1) % BS +
-                  BS * ((pgy - 1) % BS) + BS * BS * ((pgz - 1) % BS);
-    }
+  const int px0 = (int)floorf(pxc), py0 = (int)floorf(pyc), pz0 = (int)floorf(pzc);
+  wx = pxc - (float)px0;
+  wy = pyc - (float)py0;
+  wz = pzc - (float)pz0;
+  const int pgx = (s & 1) ? px0 + 1 : max(1, px0);
+  const int pgy = (s & 2) ? py0 + 1 : max(1, py0);
+  const int pgz = (s & 4) ? pz0 + 1 : max(1, pz0);
+  const int pbx = (pgx - 1) / BS + 1, pby = (pgy - 1) / BS + 1, pbz = (pgz - 1) / BS + 1;
+  if (pbx >= 1 && pbx <= L.pdim_x && pby >= 1 && pby <= L.pdim_y && pbz >= 1 &&
+      pbz <= L.pdim_z) {
+    const int pb = L.pptr[(pbx - 1) + L.pdim_x * ((pby - 1) + L.pdim_y * (pbz - 1))];
+    if (pb > 0)
+      return (int64_t)(L.p_block_offset + pb - 1) * BCELLS + (pgx - 1) % BS +
+             BS * ((pgy - 1) % BS) + BS * BS * ((pgz - 1) % BS);
   }
+  return -1;
+}
+
+template <class DEV>
+__device__ __forceinline__ void parent_stencil(const DEV &L, int gx, int gy, int gz,
+                                               ParentStencil &P) {
+#pragma unroll
+  for (int s = 0; s < 8; ++s) P.ci[s] = parent_corner(L, gx, gy, gz, s, P.wx, P.wy, P.wz);
 }
 
 // a * (1 - w) + b * w, each product and the sum rounded on its own (as the
@@ -649,6 +654,10 @@ __device__ __forceinline__ float *ghost_next_row_of(const DEV &L, int b) {
 // What the ghost pass needs to know of a flow level; the thermal DDF
 // provides the same functions for its populations (thermal.cuh).
 __device__ __forceinline__ const ol_step_params &ghost_params(const LevelDev &L) { return L.sp; }
+__device__ __forceinline__ void ghost_corner_moments(const LevelDev &L, int64_t c, float tw,
+                                                     float (&m)[4]) {
+  corner_moments(L, c, tw, m);
+}
 __device__ __forceinline__ void ghost_moments(const LevelDev &L, const ParentStencil &P, float tw,
                                               float (&r)[4]) {
   interp_moments(L, P, tw, r);

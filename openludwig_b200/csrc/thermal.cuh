@@ -36,29 +36,36 @@ struct ThermalDev {
 __device__ __forceinline__ const ol_thermal_params &ghost_params(const ThermalDev &D) {
   return D.tp;
 }
+// Blended parent T, ux, uy, uz of the present parent cell c at weight tw.
+__device__ __forceinline__ void ghost_corner_moments(const ThermalDev &D, int64_t c, float tw,
+                                                     float (&m)[4]) {
+  const bool temporal = D.tp.use_temporal_interp == 1 && tw < 0.99f;
+  const int64_t S = D.p_dstride;
+  if (temporal && tw == 0.0f) {   // old state alone (blend_parent)
+    m[0] = D.pT_old[c]; m[1] = D.pvel_old[c]; m[2] = D.pvel_old[c + S];
+    m[3] = D.pvel_old[c + 2 * S];
+    return;
+  }
+  const float Tn = D.pT[c], uxn = D.pvel[c], uyn = D.pvel[c + S], uzn = D.pvel[c + 2 * S];
+  if (temporal) {
+    m[0] = lerp_rn(D.pT_old[c], Tn, tw);
+    m[1] = lerp_rn(D.pvel_old[c], uxn, tw);
+    m[2] = lerp_rn(D.pvel_old[c + S], uyn, tw);
+    m[3] = lerp_rn(D.pvel_old[c + 2 * S], uzn, tw);
+  } else {
+    m[0] = Tn; m[1] = uxn; m[2] = uyn; m[3] = uzn;
+  }
+}
+
 __device__ __forceinline__ void ghost_moments(const ThermalDev &D, const ParentStencil &P,
                                               float tw, float (&r)[4]) {
-  const bool temporal = D.tp.use_temporal_interp == 1 && tw < 0.99f;
   float v[4][8];
 #pragma unroll
   for (int s = 0; s < 8; ++s) {
-    v[0][s] = 1.0f; v[1][s] = 0.0f; v[2][s] = 0.0f; v[3][s] = 0.0f;
-    const int64_t c = P.ci[s];
-    if (c >= 0 && temporal && tw == 0.0f) {   // old state alone (blend_parent)
-      v[0][s] = D.pT_old[c]; v[1][s] = D.pvel_old[c];
-      v[2][s] = D.pvel_old[c + D.p_dstride]; v[3][s] = D.pvel_old[c + 2 * D.p_dstride];
-    } else if (c >= 0) {
-      const float Tn = D.pT[c], uxn = D.pvel[c], uyn = D.pvel[c + D.p_dstride],
-                  uzn = D.pvel[c + 2 * D.p_dstride];
-      if (temporal) {
-        v[0][s] = lerp_rn(D.pT_old[c], Tn, tw);
-        v[1][s] = lerp_rn(D.pvel_old[c], uxn, tw);
-        v[2][s] = lerp_rn(D.pvel_old[c + D.p_dstride], uyn, tw);
-        v[3][s] = lerp_rn(D.pvel_old[c + 2 * D.p_dstride], uzn, tw);
-      } else {
-        v[0][s] = Tn; v[1][s] = uxn; v[2][s] = uyn; v[3][s] = uzn;
-      }
-    }
+    float m[4] = {1.0f, 0.0f, 0.0f, 0.0f};
+    if (P.ci[s] >= 0) ghost_corner_moments(D, P.ci[s], tw, m);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) v[i][s] = m[i];
   }
 #pragma unroll
   for (int s = 1; s < 8; ++s)
