@@ -324,26 +324,36 @@ def main():
     rate, dt_ms = replicas.job_rate(upd * nsteps, e0.elapsed_time(e1), dev)
     value = rate / 1e6
 
-    # e2e: reference-facing C-ABI calls per level sub-step + per-step D2H of diagnostics
+    # e2e: reference-facing C-ABI calls per level sub-step (step parameters
+    # passed from the host each call) + a device-to-host read of the step's
+    # FP64 flow statistics every step, into pinned memory, double-buffered:
+    # a buffer is reused only after its copy (two steps earlier) has landed
     nb = hosts[0].n_blocks
     partials = torch.empty(int(N.lib().ol_flow_stats_scratch_doubles(nb)), dtype=torch.float64, device=dev)
-    out7 = (__import__("ctypes").c_double * 7)()
+    dev7 = torch.empty((2, 7), dtype=torch.float64, device=dev)
+    host7 = torch.empty((2, 7), dtype=torch.float64, pin_memory=True)
+    landed = [torch.cuda.Event(), torch.cuda.Event()]
     import ctypes as C
     ke = max(2, a.steps // 2)
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
-    t0 = time.perf_counter()
     with torch.cuda.stream(stream):
         ee0, ee1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         ee0.record(stream)
-        for _ in range(ke):
+        for i in range(ke):
             state["t"] += 1
             coarse_step(state["t"])
             lv0 = levels[0]
             vel = lv0.vel if state["t"] % 2 == 1 else lv0.vel_temp
-            N.call("ol_flow_stats", S._ptr(lv0.rho), S._ptr(vel), S._ptr(lv0.obstacle), N.i32(nb),
-                   S._ptr(partials), out7, C.c_void_p(stream.cuda_stream))
+            slot = i % 2
+            if i >= 2:
+                landed[slot].synchronize()
+                assert host7[slot, 0].item() > 0       # the statistics of step i - 2 arrived
+            N.call("ol_flow_stats_device", S._ptr(lv0.rho), S._ptr(vel), S._ptr(lv0.obstacle),
+                   N.i32(nb), S._ptr(partials), S._ptr(dev7[slot]), C.c_void_p(stream.cuda_stream))
+            host7[slot].copy_(dev7[slot], non_blocking=True)
+            landed[slot].record(stream)
         ee1.record(stream)
     torch.cuda.synchronize()
     e2e_rate, e2e_ms = replicas.job_rate(upd * ke, ee0.elapsed_time(ee1), dev)

@@ -86,10 +86,11 @@ typedef struct ol_level_view {
   float *ghost_next;
   int32_t ghost_mode;
   /* Optional [n_ghost_blocks] 0-based ids of the blocks the ghost pass visits
-   * (NULL = every block; the pass skips blocks without an absent neighbour).
-   * A list must hold every block with an absent neighbour, or under
-   * OL_GHOST_PAIR_SECOND every block with an absent neighbour not wholly
-   * inside the level's domain; it saves the launch of the other blocks. */
+   * (NULL = every block; the pass skips blocks without an absent neighbour;
+   * a non-NULL list with n_ghost_blocks = 0 launches no pass).  A list must
+   * hold every block with an absent neighbour, or under OL_GHOST_PAIR_SECOND
+   * every block with an absent neighbour not wholly inside the level's
+   * domain; it saves the launch of the other blocks. */
   const int32_t *ghost_blocks;
   int32_t n_ghost_blocks;
 } ol_level_view;
@@ -282,6 +283,12 @@ OL_API int ol_flow_stats(const float *rho, const float *vel, const uint8_t *obst
                   int32_t n_blocks, double *partials, double out[7],
                   void *stream);
 OL_API size_t ol_flow_stats_scratch_doubles(int32_t n_blocks);
+/* The same statistics into out7_dev (7 doubles of device memory), enqueued
+ * on `stream` without waiting: for a driver that reads them back
+ * asynchronously (a copy to pinned memory it checks a step later). */
+OL_API int ol_flow_stats_device(const float *rho, const float *vel, const uint8_t *obstacle,
+                         int32_t n_blocks, double *partials, double *out7_dev,
+                         void *stream);
 
 /* ------------------------------------------------------------------ */
 /* Native layer: device block pool, FP16-shifted storage, batched       */

@@ -151,6 +151,7 @@ _SIGS = {
                                         vp]),
     "ol_flow_stats": (C.c_int, [vp, vp, vp, i32, vp, C.POINTER(C.c_double), vp]),
     "ol_flow_stats_scratch_doubles": (C.c_size_t, [i32]),
+    "ol_flow_stats_device": (C.c_int, [vp, vp, vp, i32, vp, vp, vp]),
     "ol_ghost_floats": (C.c_int64, [i32]),
     "ol_ctx_create": (C.c_int, [C.POINTER(vp), C.c_int, C.c_size_t, C.c_int]),
     "ol_ctx_destroy": (C.c_int, [vp]),

@@ -377,6 +377,17 @@ extern "C" int ol_surface_net_forces(const ol_surface_mesh *mesh, const float *r
   return OL_OK;
 }
 
+extern "C" int ol_flow_stats_device(const float *rho, const float *vel, const uint8_t *obstacle,
+                                    int32_t n_blocks, double *partials, double *out7_dev,
+                                    void *stream) {
+  OL_CHECK_ARG(n_blocks > 0 && rho && vel && obstacle && partials && out7_dev,
+               "ol_flow_stats_device: bad argument");
+  launch_flow_stats(rho, vel, obstacle, n_blocks, 0, (int64_t)BCELLS * n_blocks, partials,
+                    out7_dev, (cudaStream_t)stream);
+  OL_LAUNCHED("ol_flow_stats_device");
+  return OL_OK;
+}
+
 extern "C" size_t ol_flow_stats_scratch_doubles(int32_t n_blocks) {
   return (size_t)(n_blocks > 0 ? n_blocks : 0) * 7 + 8;
 }

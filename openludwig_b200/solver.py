@@ -75,7 +75,8 @@ class DeviceLevel:
     ghost2: torch.Tensor | None = None
     ghost_g2: torch.Tensor | None = None
     # blocks the ghost pass visits: those with an absent neighbour, and those
-    # with one not wholly inside the domain (second sub-step of a pair)
+    # with one not wholly inside the domain (second sub-step of a pair); each
+    # list ends with one unused entry
     ghost_list: torch.Tensor | None = None
     edge_list: torch.Tensor | None = None
     # thermal DDF
@@ -277,7 +278,7 @@ def _ghost_views(view, lv: DeviceLevel, ghost, ghost2, mode: int) -> None:
     view.ghost_next = _ptr(ghost2) if mode == N.OL_GHOST_PAIR_FIRST else None
     lst = lv.edge_list if mode == N.OL_GHOST_PAIR_SECOND else lv.ghost_list
     if ghost is not None and lst is not None:
-        view.ghost_blocks, view.n_ghost_blocks = _ptr(lst), int(lst.numel())
+        view.ghost_blocks, view.n_ghost_blocks = _ptr(lst), int(lst.numel()) - 1
 
 
 def perform_timestep(s: StepSettings, lv: DeviceLevel, parent: ParentRef | None, f_out, f_in,
@@ -294,9 +295,11 @@ def perform_timestep(s: StepSettings, lv: DeviceLevel, parent: ParentRef | None,
     dims = (domain_dims[0] * scale, domain_dims[1] * scale, domain_dims[2] * scale)
     ref_post = lv.f_post is not None
     if lv.ghost is not None and lv.ghost_list is None:   # static: computed on first use
+        # one trailing entry keeps an empty list's pointer non-null (a null
+        # list means "every block"); the view passes the true length
         gl, el = ghost_block_lists(lv.host, dims)
-        lv.ghost_list = torch.from_numpy(gl).to(lv.f.device)
-        lv.edge_list = torch.from_numpy(el).to(lv.f.device)
+        lv.ghost_list = torch.from_numpy(np.append(gl, -1).astype(np.int32)).to(lv.f.device)
+        lv.edge_list = torch.from_numpy(np.append(el, -1).astype(np.int32)).to(lv.f.device)
     sp = step_params(s, lv, parent.lv.tau if parent else 0.5, is_l1, dims, u, t_sub, tw,
                      lv.has_bouzidi and ref_post)
     view = N.LevelView(f_out=_ptr(f_out), f_in=_ptr(f_in), f_post=_ptr(lv.f_post),

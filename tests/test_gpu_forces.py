@@ -93,3 +93,37 @@ def test_net_forces_match_oracle_on_open_plate(closed):
         assert np.allclose(tot, ref, rtol=1e-4, atol=1e-4 * np.abs(ref).max())
     else:
         assert minus_cover > 0.8 * sim.dmesh.n
+
+
+def test_flow_stats_match_numpy_fp64():
+    """compute_flow_stats (diagnostics.jl:43-93) in FP64 against numpy on the
+    same device state; the asynchronous entry point gives the same bits."""
+    import ctypes as C
+    from openludwig_b200 import _native as N
+    c, mesh, p, hosts = small_sphere_case(resolution=8)
+    c.ramp_steps = 0
+    sim = S.Simulation(c, mesh, p, hosts, DEV)
+    sim.run(20, diag_freq=20)
+    lv = sim.levels[0]
+    st = S.flow_stats(lv)
+    torch.cuda.synchronize()
+    rho = lv.rho.cpu().numpy().astype(np.float64)
+    vel = lv.vel.cpu().numpy().astype(np.float64).reshape(3, -1)
+    fluid = lv.obstacle.cpu().numpy() == 0
+    v2 = (vel ** 2).sum(axis=0)
+    assert st["n_fluid"] == int(fluid.sum())
+    assert st["rho_mean"] == pytest.approx(rho[fluid].mean(), rel=1e-12)
+    assert st["rho_min"] == rho[fluid].min() and st["rho_max"] == rho[fluid].max()
+    assert st["v_max"] == pytest.approx(np.sqrt(v2[fluid]).max(), rel=1e-15)
+    assert st["kinetic_energy"] == pytest.approx((0.5 * rho * v2)[fluid].sum(), rel=1e-12)
+    assert st["mass"] == pytest.approx(rho.sum(), rel=1e-12)
+    nb = lv.n_blocks
+    partials = torch.empty(int(N.lib().ol_flow_stats_scratch_doubles(nb)), dtype=torch.float64,
+                           device=DEV)
+    out = (C.c_double * 7)()
+    N.call("ol_flow_stats", S._ptr(lv.rho), S._ptr(lv.vel), S._ptr(lv.obstacle), N.i32(nb),
+           S._ptr(partials), out, S._stream())
+    dev7 = torch.empty(7, dtype=torch.float64, device=DEV)
+    N.call("ol_flow_stats_device", S._ptr(lv.rho), S._ptr(lv.vel), S._ptr(lv.obstacle), N.i32(nb),
+           S._ptr(partials), S._ptr(dev7), S._stream())
+    assert dev7.cpu().numpy().tolist() == list(out)
