@@ -33,6 +33,10 @@ static std::vector<uint32_t> build_halo_table() {
     if (x >= 0 && x < 8 && y >= 0 && y < 8 && z >= 0 && z < 8) continue;
     tab.push_back((uint32_t)p);
   }
+  // then, per halo entry, the ring index of its staging slot
+  std::vector<int> ring_of(1000, -1);
+  for (int q = 0; q < kRingEntries; ++q) ring_of[tab[kHaloEntries + q]] = q;
+  for (int i = 0; i < kHaloEntries; ++i) tab.push_back((uint32_t)ring_of[tab[i] >> 19]);
   return tab;
 }
 
@@ -44,7 +48,7 @@ const uint32_t *halo_table_device() {
   std::lock_guard<std::mutex> lk(mu);
   if (!per_dev[dev]) {
     const std::vector<uint32_t> tab = build_halo_table();
-    if ((int)tab.size() != kHaloEntries + kRingEntries) return nullptr;
+    if ((int)tab.size() != kHaloTableSize) return nullptr;
     uint32_t *d = nullptr;
     if (cudaMalloc(&d, tab.size() * sizeof(uint32_t)) != cudaSuccess) return nullptr;
     if (cudaMemcpy(d, tab.data(), tab.size() * sizeof(uint32_t), cudaMemcpyHostToDevice) !=

@@ -19,8 +19,10 @@ namespace ol {
 // blended, interpolated rho and u) and the per-direction population.
 // gx, gy, gz: 1-based fine-level global source coordinates.
 // ---------------------------------------------------------------------------
+// Parent cell indices fit 32 bits (every launch checks that a level's cells
+// do); gathers add them to per-plane base pointers.
 struct ParentStencil {
-  int64_t ci[8];     // parent cell of each trilinear corner, -1 when absent
+  int32_t ci[8];     // parent cell of each trilinear corner, -1 when absent
   float wx, wy, wz;  // trilinear weights
 };
 
@@ -28,7 +30,7 @@ struct ParentStencil {
 // parent cell of corner s (bit 0: x + 1, bit 1: y + 1, bit 2: z + 1), or -1
 // when that parent cell does not exist.
 template <class DEV>
-__device__ __forceinline__ int64_t parent_corner(const DEV &L, int gx, int gy, int gz, int s,
+__device__ __forceinline__ int32_t parent_corner(const DEV &L, int gx, int gy, int gz, int s,
                                                  float &wx, float &wy, float &wz) {
   const float pxc = ((float)gx - 0.5f) * 0.5f;
   const float pyc = ((float)gy - 0.5f) * 0.5f;
@@ -45,7 +47,7 @@ __device__ __forceinline__ int64_t parent_corner(const DEV &L, int gx, int gy, i
       pbz <= L.pdim_z) {
     const int pb = L.pptr[(pbx - 1) + L.pdim_x * ((pby - 1) + L.pdim_y * (pbz - 1))];
     if (pb > 0)
-      return (int64_t)(L.p_block_offset + pb - 1) * BCELLS + (pgx - 1) % BS +
+      return (int32_t)((L.p_block_offset + pb - 1) * BCELLS) + (pgx - 1) % BS +
              BS * ((pgy - 1) % BS) + BS * BS * ((pgz - 1) % BS);
   }
   return -1;
@@ -87,21 +89,22 @@ __device__ __forceinline__ float blend_parent(bool temporal, float tw, float old
 
 // Blended parent moments (rho, ux, uy, uz) of the present parent cell c at
 // temporal weight tw.
-__device__ __forceinline__ void corner_moments(const LevelDev &L, int64_t c, float tw,
+__device__ __forceinline__ void corner_moments(const LevelDev &L, uint32_t c, float tw,
                                                float (&m)[4]) {
   const bool temporal = L.sp.use_temporal_interp == 1 && tw < 0.99f;
   const int64_t S = L.p_dstride;
+  const float *vo = L.pvel_old, *vn = L.pvel;
   if (temporal && tw == 0.0f) {
-    m[0] = L.prho_old[c]; m[1] = L.pvel_old[c];
-    m[2] = L.pvel_old[c + S]; m[3] = L.pvel_old[c + 2 * S];
+    m[0] = L.prho_old[c]; m[1] = vo[c];
+    m[2] = (vo + S)[c]; m[3] = (vo + 2 * S)[c];
     return;
   }
-  const float rn = L.prho[c], uxn = L.pvel[c], uyn = L.pvel[c + S], uzn = L.pvel[c + 2 * S];
+  const float rn = L.prho[c], uxn = vn[c], uyn = (vn + S)[c], uzn = (vn + 2 * S)[c];
   if (temporal) {
     m[0] = lerp_rn(L.prho_old[c], rn, tw);
-    m[1] = lerp_rn(L.pvel_old[c], uxn, tw);
-    m[2] = lerp_rn(L.pvel_old[c + S], uyn, tw);
-    m[3] = lerp_rn(L.pvel_old[c + 2 * S], uzn, tw);
+    m[1] = lerp_rn(vo[c], uxn, tw);
+    m[2] = lerp_rn((vo + S)[c], uyn, tw);
+    m[3] = lerp_rn((vo + 2 * S)[c], uzn, tw);
   } else {
     m[0] = rn; m[1] = uxn; m[2] = uyn; m[3] = uzn;
   }
@@ -109,14 +112,14 @@ __device__ __forceinline__ void corner_moments(const LevelDev &L, int64_t c, flo
 
 // Blended parent population k of the present parent cell c at weight tw.
 template <class ST>
-__device__ __forceinline__ float corner_population(const LevelDev &L, int64_t c, int k,
+__device__ __forceinline__ float corner_population(const LevelDev &L, uint32_t c, int k,
                                                    float tw) {
   const bool temporal = L.sp.use_temporal_interp == 1 && tw < 0.99f;
-  const size_t a = (size_t)c + (size_t)k * L.p_dstride;
   using T = typename ST::T;
-  const float fo = temporal ? ST::load((const T *)L.pf_old, a, k, L.p_inv_scale) : 0.0f;
-  return blend_parent(temporal, tw, fo,
-                      [&] { return ST::load((const T *)L.pf, a, k, L.p_inv_scale); });
+  const T *po = (const T *)L.pf_old + (size_t)k * L.p_dstride;   // plane k
+  const T *pn = (const T *)L.pf + (size_t)k * L.p_dstride;
+  const float fo = temporal ? ST::load(po, c, k, L.p_inv_scale) : 0.0f;
+  return blend_parent(temporal, tw, fo, [&] { return ST::load(pn, c, k, L.p_inv_scale); });
 }
 
 // Parent rho, ux, uy, uz at the ghost position: each corner blended between
@@ -128,7 +131,7 @@ __device__ __forceinline__ void interp_moments(const LevelDev &L, const ParentSt
 #pragma unroll
   for (int s = 0; s < 8; ++s) {
     float m[4] = {1.0f, 0.0f, 0.0f, 0.0f};
-    if (P.ci[s] >= 0) corner_moments(L, P.ci[s], tw, m);
+    if (P.ci[s] >= 0) corner_moments(L, (uint32_t)P.ci[s], tw, m);
 #pragma unroll
     for (int i = 0; i < 4; ++i) v[i][s] = m[i];
   }
@@ -166,7 +169,7 @@ __device__ __forceinline__ float interp_population(const LevelDev &L, int k,
   float v[8];
 #pragma unroll
   for (int s = 0; s < 8; ++s)
-    v[s] = P.ci[s] >= 0 ? corner_population<ST>(L, P.ci[s], k, tw) : w_of(k);
+    v[s] = P.ci[s] >= 0 ? corner_population<ST>(L, (uint32_t)P.ci[s], k, tw) : w_of(k);
 #pragma unroll
   for (int s = 1; s < 8; ++s)
     if (P.ci[s] < 0) v[s] = v[0];
@@ -185,14 +188,16 @@ __device__ __forceinline__ void interp_population_pair(const LevelDev &L, int k,
                                                        float &g1) {
   const bool temporal = L.sp.use_temporal_interp == 1;
   using T = typename ST::T;
+  const T *po = (const T *)L.pf_old + (size_t)k * L.p_dstride;   // plane k
+  const T *pn = (const T *)L.pf + (size_t)k * L.p_dstride;
   float v0[8], v1[8];
 #pragma unroll
   for (int s = 0; s < 8; ++s) {
     v0[s] = v1[s] = w_of(k);
     if (P.ci[s] >= 0) {
-      const size_t a = (size_t)P.ci[s] + (size_t)k * L.p_dstride;
-      const float fn = ST::load((const T *)L.pf, a, k, L.p_inv_scale);
-      const float fo = temporal ? ST::load((const T *)L.pf_old, a, k, L.p_inv_scale) : fn;
+      const uint32_t c = (uint32_t)P.ci[s];
+      const float fn = ST::load(pn, c, k, L.p_inv_scale);
+      const float fo = temporal ? ST::load(po, c, k, L.p_inv_scale) : fn;
       v0[s] = fo;
       v1[s] = temporal ? lerp_rn(fo, fn, kSecondSubstepWeight) : fn;
     }
@@ -535,6 +540,10 @@ __device__ __noinline__ void fill_missing_slots(const int *nbbase, int t, float 
 // Ring positions of the staging plane (the 488 slots of the 10^3 plane
 // outside the 8^3 block), listed in the staging table after its halo entries.
 constexpr int kRingEntries = 1000 - 512;
+// Staging table layout: kHaloEntries packed entries, the kRingEntries ring
+// slots of the 10^3 plane, then per halo entry the ring index of its slot.
+constexpr int kRingIndexOffset = kHaloEntries + kRingEntries;
+constexpr int kHaloTableSize = kRingIndexOffset + kHaloEntries;
 
 // Staging planes whose slot p is never read, for a ring position p with
 // outward offsets (ox, oy, oz): a direction k with c_a = o_a on the first
@@ -654,7 +663,7 @@ __device__ __forceinline__ float *ghost_next_row_of(const DEV &L, int b) {
 // What the ghost pass needs to know of a flow level; the thermal DDF
 // provides the same functions for its populations (thermal.cuh).
 __device__ __forceinline__ const ol_step_params &ghost_params(const LevelDev &L) { return L.sp; }
-__device__ __forceinline__ void ghost_corner_moments(const LevelDev &L, int64_t c, float tw,
+__device__ __forceinline__ void ghost_corner_moments(const LevelDev &L, uint32_t c, float tw,
                                                      float (&m)[4]) {
   corner_moments(L, c, tw, m);
 }
@@ -693,7 +702,7 @@ __device__ __forceinline__ void ghost_fill_block(const DEV &L, int b, float *G, 
   __shared__ float rs2[4][kRingEntries];    // the same at the second sub-step's weight
   __shared__ int32_t cs[8][kRingEntries];   // parent stencil cells
   __shared__ float ws[3][kRingEntries];     // trilinear weights
-  __shared__ int16_t ring_of[EPL];          // staging slot -> ring index
+  __shared__ uint8_t iface_of[kRingEntries];  // ring position takes coarse-to-fine values
   __shared__ int16_t pos_list[kRingEntries];
   __shared__ int16_t slot_list[kHaloEntries];
   const int t = threadIdx.x;
@@ -732,21 +741,21 @@ __device__ __forceinline__ void ghost_fill_block(const DEV &L, int b, float *G, 
     const int i = t + j * kGhostThreads;
     te[j] = i < kHaloEntries ? __ldg(tab + i) : 0u;
   }
-  if (interp) {
+  if (fine) {
     for (int j = 0; j < (kRingEntries + kGhostThreads - 1) / kGhostThreads; ++j) {
       const int q = t + j * kGhostThreads;
       bool want = false;
       if (q < kRingEntries) {
         const int p = (int)__ldg(tab + kHaloEntries + q);
-        ring_of[p] = (int16_t)q;
         const int sx = p % 10 - 1, sy = (p / 10) % 10 - 1, sz = p / 100 - 1;
         const int ox = sx < 0 ? -1 : (sx > 7 ? 1 : 0);
         const int oy = sy < 0 ? -1 : (sy > 7 ? 1 : 0);
         const int oz = sz < 0 ? -1 : (sz > 7 ? 1 : 0);
         want = nbbase[(ox + 1) + 3 * (oy + 1) + 9 * (oz + 1)] < 0 &&
                in_domain(gx0 + sx, gy0 + sy, gz0 + sz);
+        iface_of[q] = want;
       }
-      append_if(want, q, &n_pos, pos_list);
+      append_if(interp && want, q, &n_pos, pos_list);
     }
   }
 #pragma unroll
@@ -772,7 +781,7 @@ __device__ __forceinline__ void ghost_fill_block(const DEV &L, int b, float *G, 
         for (int i = 0; i < 4; ++i) rs2[i][q] = r[i];
       }
 #pragma unroll
-      for (int s = 0; s < 8; ++s) cs[s][q] = (int32_t)P.ci[s];
+      for (int s = 0; s < 8; ++s) cs[s][q] = P.ci[s];
       ws[0][q] = P.wx; ws[1][q] = P.wy; ws[2][q] = P.wz;
     }
     __syncthreads();
@@ -780,11 +789,10 @@ __device__ __forceinline__ void ghost_fill_block(const DEV &L, int b, float *G, 
   for (int j = t; j < n_slot; j += kGhostThreads) {
     const int i = slot_list[j];
     const uint32_t e = __ldg(tab + i);
-    const int k = e & 31, p = e >> 19;
-    const int sx = p % 10 - 1, sy = (p / 10) % 10 - 1, sz = p / 100 - 1;
-    if (fine && in_domain(gx0 + sx, gy0 + sy, gz0 + sz)) {
+    const int k = e & 31;
+    const int q = fine ? (int)__ldg(tab + kRingIndexOffset + i) : 0;
+    if (fine && iface_of[q]) {
       if (precomputed) continue;
-      const int q = ring_of[p];
       ParentStencil P;
 #pragma unroll
       for (int s = 0; s < 8; ++s) P.ci[s] = cs[s][q];
@@ -800,6 +808,8 @@ __device__ __forceinline__ void ghost_fill_block(const DEV &L, int b, float *G, 
         G[i] = ghost_population(L, k, P, r, tw, ST{});
       }
     } else {
+      const int p = e >> 19;
+      const int sx = p % 10 - 1, sy = (p / 10) % 10 - 1, sz = p / 100 - 1;
       G[i] = ghost_boundary(L, k, b, sx + cx_of(k), sy + cy_of(k), sz + cz_of(k), ST{});
     }
   }

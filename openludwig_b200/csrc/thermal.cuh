@@ -37,21 +37,21 @@ __device__ __forceinline__ const ol_thermal_params &ghost_params(const ThermalDe
   return D.tp;
 }
 // Blended parent T, ux, uy, uz of the present parent cell c at weight tw.
-__device__ __forceinline__ void ghost_corner_moments(const ThermalDev &D, int64_t c, float tw,
+__device__ __forceinline__ void ghost_corner_moments(const ThermalDev &D, uint32_t c, float tw,
                                                      float (&m)[4]) {
   const bool temporal = D.tp.use_temporal_interp == 1 && tw < 0.99f;
   const int64_t S = D.p_dstride;
+  const float *vo = D.pvel_old, *vn = D.pvel;
   if (temporal && tw == 0.0f) {   // old state alone (blend_parent)
-    m[0] = D.pT_old[c]; m[1] = D.pvel_old[c]; m[2] = D.pvel_old[c + S];
-    m[3] = D.pvel_old[c + 2 * S];
+    m[0] = D.pT_old[c]; m[1] = vo[c]; m[2] = (vo + S)[c]; m[3] = (vo + 2 * S)[c];
     return;
   }
-  const float Tn = D.pT[c], uxn = D.pvel[c], uyn = D.pvel[c + S], uzn = D.pvel[c + 2 * S];
+  const float Tn = D.pT[c], uxn = vn[c], uyn = (vn + S)[c], uzn = (vn + 2 * S)[c];
   if (temporal) {
     m[0] = lerp_rn(D.pT_old[c], Tn, tw);
-    m[1] = lerp_rn(D.pvel_old[c], uxn, tw);
-    m[2] = lerp_rn(D.pvel_old[c + S], uyn, tw);
-    m[3] = lerp_rn(D.pvel_old[c + 2 * S], uzn, tw);
+    m[1] = lerp_rn(vo[c], uxn, tw);
+    m[2] = lerp_rn((vo + S)[c], uyn, tw);
+    m[3] = lerp_rn((vo + 2 * S)[c], uzn, tw);
   } else {
     m[0] = Tn; m[1] = uxn; m[2] = uyn; m[3] = uzn;
   }
@@ -63,7 +63,7 @@ __device__ __forceinline__ void ghost_moments(const ThermalDev &D, const ParentS
 #pragma unroll
   for (int s = 0; s < 8; ++s) {
     float m[4] = {1.0f, 0.0f, 0.0f, 0.0f};
-    if (P.ci[s] >= 0) ghost_corner_moments(D, P.ci[s], tw, m);
+    if (P.ci[s] >= 0) ghost_corner_moments(D, (uint32_t)P.ci[s], tw, m);
 #pragma unroll
     for (int i = 0; i < 4; ++i) v[i][s] = m[i];
   }
@@ -94,17 +94,17 @@ __device__ __forceinline__ float ghost_population(const ThermalDev &D, int k,
                                                   const ParentStencil &P, const float (&r)[4],
                                                   float tw, ST) {
   const bool temporal = D.tp.use_temporal_interp == 1 && tw < 0.99f;
+  using T = typename ST::T;
+  const T *po = (const T *)D.pg_old + (size_t)k * D.p_dstride;   // plane k
+  const T *pn = (const T *)D.pg + (size_t)k * D.p_dstride;
   float v[8];
 #pragma unroll
   for (int s = 0; s < 8; ++s) {
     v[s] = w_of(k);
-    const int64_t c = P.ci[s];
-    if (c >= 0) {
-      const size_t a = (size_t)c + (size_t)k * D.p_dstride;
-      using T = typename ST::T;
-      const float go = temporal ? ST::load((const T *)D.pg_old, a, k, D.p_inv_scale) : 0.0f;
-      v[s] = blend_parent(temporal, tw, go,
-                          [&] { return ST::load((const T *)D.pg, a, k, D.p_inv_scale); });
+    if (P.ci[s] >= 0) {
+      const uint32_t c = (uint32_t)P.ci[s];
+      const float go = temporal ? ST::load(po, c, k, D.p_inv_scale) : 0.0f;
+      v[s] = blend_parent(temporal, tw, go, [&] { return ST::load(pn, c, k, D.p_inv_scale); });
     }
   }
 #pragma unroll
@@ -122,15 +122,16 @@ __device__ __forceinline__ void ghost_population_pair(const ThermalDev &D, int k
                                                       ST, float &g0, float &g1) {
   const bool temporal = D.tp.use_temporal_interp == 1;
   using T = typename ST::T;
+  const T *po = (const T *)D.pg_old + (size_t)k * D.p_dstride;   // plane k
+  const T *pn = (const T *)D.pg + (size_t)k * D.p_dstride;
   float v0[8], v1[8];
 #pragma unroll
   for (int s = 0; s < 8; ++s) {
     v0[s] = v1[s] = w_of(k);
-    const int64_t c = P.ci[s];
-    if (c >= 0) {
-      const size_t a = (size_t)c + (size_t)k * D.p_dstride;
-      const float gn = ST::load((const T *)D.pg, a, k, D.p_inv_scale);
-      const float go = temporal ? ST::load((const T *)D.pg_old, a, k, D.p_inv_scale) : gn;
+    if (P.ci[s] >= 0) {
+      const uint32_t c = (uint32_t)P.ci[s];
+      const float gn = ST::load(pn, c, k, D.p_inv_scale);
+      const float go = temporal ? ST::load(po, c, k, D.p_inv_scale) : gn;
       v0[s] = go;
       v1[s] = temporal ? lerp_rn(go, gn, kSecondSubstepWeight) : gn;
     }
