@@ -77,6 +77,7 @@ struct LevelDev {
   int32_t ghost_mode;
   const int32_t *gblocks;  // blocks the drop-in ghost pass visits (null = all)
   int32_t n_gblocks;
+  int32_t prefetch_ahead;  // stream-collide: L2-prefetch block b + this (0 = off)
 };
 
 constexpr int kGhostUnpaired = 0, kGhostPairFirst = 1, kGhostPairSecond = 2;

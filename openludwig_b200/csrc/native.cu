@@ -143,6 +143,10 @@ __global__ void __launch_bounds__(512, OP == OL_OP_CUMULANT ? 2 : 1)
     const WorkItem w = items[it];
     copy_desc(&L, descs + w.desc, t);
     if (DDF) copy_desc(&D, tdescs + w.desc, t);
+    if (it + (int)gridDim.x < n_items && t < 33) {  // this CTA's next item, into L2
+      const WorkItem w2 = items[it + gridDim.x];
+      prefetch_block_l2<ST>(descs[w2.desc], w2.block, t);
+    }
     __syncthreads();
     const int64_t own0 = (L.block_offset + w.block) * BCELLS;
     OwnRegs<ST> r;

@@ -74,6 +74,7 @@ __global__ void __launch_bounds__(512, OP == OL_OP_CUMULANT ? 2 : 1)
   // the own block's planes and masks do not depend on the neighbour table:
   // their loads are in flight while it is read
   const int64_t own0 = (L.block_offset + b) * BCELLS;
+  if (L.prefetch_ahead > 0) prefetch_block_l2<ST>(L, b + L.prefetch_ahead, threadIdx.x);
   OwnRegs<ST> r;
   own_load(L.f_in, L.dstride, own0, threadIdx.x, r);
   const bool obs = L.obstacle[own0 + threadIdx.x] != 0;
@@ -85,13 +86,24 @@ __global__ void __launch_bounds__(512, OP == OL_OP_CUMULANT ? 2 : 1)
 }
 
 template <int OP, class ST, bool WALE>
-static void launch_one(const LevelDev &L, cudaStream_t s) {
+static void launch_one(const LevelDev &L0, cudaStream_t s) {
   static bool done = false;
+  static int resident = 0;  // CTAs of this kernel resident on the whole device
   if (!done) {
     cudaFuncSetAttribute(k_stream_collide<OP, ST, WALE>,
                          cudaFuncAttributeMaxDynamicSharedMemorySize, kStageBytes);
+    int dev = 0, n_sm = 0, per_sm = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess &&
+        cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess &&
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_stream_collide<OP, ST, WALE>,
+                                                      BCELLS, kStageBytes) == cudaSuccess)
+      resident = n_sm * per_sm;
     done = true;
   }
+  // CTA b prefetches the block its slot takes one wave later (b + resident);
+  // a level of fewer than four waves has little to hide and skips it
+  LevelDev L = L0;
+  L.prefetch_ahead = L.n_blocks >= 4 * resident ? resident : 0;
   k_stream_collide<OP, ST, WALE><<<L.n_blocks, BCELLS, kStageBytes, s>>>(L);
 }
 

@@ -825,6 +825,37 @@ __global__ void __launch_bounds__(kGhostThreads, kGhostMinBlocks)
 
 constexpr int kHaloPerThread = (kHaloEntries + BCELLS - 1) / BCELLS;  // 7
 
+// Asks L2 for the per-cell arrays of block nb (local index) of level L: its
+// 27 population planes, velocity (WALE reads it), sponge, mask and wall
+// distance, one bulk prefetch per thread t < 33.  The stream-collide launch
+// issues this for the block its CTA slot takes one wave later, so that
+// block's staging loads find their data in L2 (no registers, no shared
+// memory, nothing to wait for).  Every run is whole and 16-byte aligned:
+// blocks are 512 cells and the arrays' planes are whole blocks.
+template <class ST>
+__device__ __forceinline__ void prefetch_block_l2(const LevelDev &L, int nb, int t) {
+  if (nb >= L.n_blocks || t >= 33) return;
+  using T = typename ST::T;
+  const int64_t o = (L.block_offset + nb) * BCELLS;
+  const void *src = nullptr;
+  unsigned bytes = BCELLS * sizeof(float);
+  if (t < 27) {
+    src = (const T *)L.f_in + o + (int64_t)t * L.dstride;
+    bytes = BCELLS * sizeof(T);
+  } else if (t < 30) {
+    if (L.vel_in) src = L.vel_in + o + (int64_t)(t - 27) * L.dstride;
+  } else if (t == 30) {
+    src = L.sponge + o;
+  } else if (t == 31) {
+    src = L.obstacle + o;
+    bytes = BCELLS;
+  } else if (L.wall_dist) {
+    src = L.wall_dist + o;
+  }
+  if (src) asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src), "r"(bytes)
+                        : "memory");
+}
+
 // The own block's 27 planes, loaded into registers with 16-byte loads
 // (FP32: 7 float4 per thread; FP16: 4 x 8 halves).  The loads depend only on
 // the block's own offset, so a kernel can issue them before it has read the
