@@ -334,7 +334,7 @@ def main():
     host7 = torch.empty((2, 7), dtype=torch.float64, pin_memory=True)
     landed = [torch.cuda.Event(), torch.cuda.Event()]
     import ctypes as C
-    ke = max(2, a.steps // 2)
+    ke = max(2, a.steps)
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()

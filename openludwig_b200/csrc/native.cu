@@ -143,7 +143,9 @@ __global__ void __launch_bounds__(512, OP == OL_OP_CUMULANT ? 2 : 1)
     const WorkItem w = items[it];
     copy_desc(&L, descs + w.desc, t);
     if (DDF) copy_desc(&D, tdescs + w.desc, t);
-    if (it + (int)gridDim.x < n_items && t < 33) {  // this CTA's next item, into L2
+    // this CTA's next item into L2 (measured: better than 3/4 of a grid ahead
+    // here, where the CTAs stay resident and walk the list in step)
+    if (it + (int)gridDim.x < n_items && t < 33) {
       const WorkItem w2 = items[it + gridDim.x];
       prefetch_block_l2<ST>(descs[w2.desc], w2.block, t);
     }

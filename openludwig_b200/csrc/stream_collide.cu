@@ -100,10 +100,12 @@ static void launch_one(const LevelDev &L0, cudaStream_t s) {
       resident = n_sm * per_sm;
     done = true;
   }
-  // CTA b prefetches the block its slot takes one wave later (b + resident);
-  // a level of fewer than four waves has little to hide and skips it
+  // CTA b prefetches a block that starts about 3/4 of a wave later (measured
+  // on the cube's finest level: 1/2 wave 261, 3/4 259, 1 263, 5/4 269 us per
+  // call; farther ahead the lines are gone again before they are staged); a
+  // level of fewer than four waves has little to hide and skips it
   LevelDev L = L0;
-  L.prefetch_ahead = L.n_blocks >= 4 * resident ? resident : 0;
+  L.prefetch_ahead = L.n_blocks >= 4 * resident ? resident * 3 / 4 : 0;
   k_stream_collide<OP, ST, WALE><<<L.n_blocks, BCELLS, kStageBytes, s>>>(L);
 }
 
