@@ -159,18 +159,11 @@ class ClockSampler:
 
 
 def build_case(workload: str):
-    from openludwig_b200 import domain, scaling, workloads
-    if workload == "cube_3lvl":
-        cfg, mesh = workloads.cube_3lvl()
-    elif workload == "sphere_1lvl":
-        cfg, mesh = workloads.sphere_1lvl()
-    elif workload == "sphere_ddf":
-        cfg, mesh = workloads.sphere_ddf()
-    else:
+    from openludwig_b200 import workloads
+    try:
+        return workloads.build_case(workload)
+    except KeyError:
         raise SystemExit(f"unknown workload {workload}")
-    p = scaling.compute_domain_from_mesh(cfg, mesh.min_bounds, mesh.max_bounds)
-    hosts = domain.setup_multilevel_domain(cfg, mesh, p)
-    return cfg, mesh, p, hosts
 
 
 def describe(workload, p, hosts) -> dict:

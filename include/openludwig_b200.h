@@ -276,6 +276,43 @@ OL_API int ol_surface_net_forces(const ol_surface_mesh *mesh, const float *rho,
                           const ol_force_params *fp, int32_t closed_body,
                           const ol_net_force_maps *out, void *stream);
 
+/* One level's part of the merged flow output (io_vtk.jl:6-129). */
+typedef struct ol_output_level {
+  const float *rho;                     /* [512*nB]                               */
+  const float *vel;                     /* [512*nB*3]: vel or vel_temp, as the
+                                           reference picks by step parity (io_vtk.jl:48) */
+  const uint8_t *obstacle;              /* [512*nB]                               */
+  const float *temperature;             /* [512*nB], or NULL without the DDF      */
+  const int32_t *map_x, *map_y, *map_z; /* [nB] 1-based block coordinates         */
+  const int32_t *blocks;                /* [n_export] 0-based ids (< nB) of the
+                                           exported blocks, in export order        */
+  int32_t n_export;
+  int32_t n_blocks;                     /* level nB (array stride)                */
+  int32_t level_id;                     /* 1-based, written to the level field    */
+  float dx;                             /* Float32(level.dx)                      */
+} ol_output_level;
+
+/* Packed output arrays (device memory), N = total exported blocks; any may
+ * be NULL to skip it.  Cell order is the block's own (x fastest), blocks
+ * level after level in list order, as the reference's VTK writer lays them. */
+typedef struct ol_output_fields {
+  float *points;       /* [3 * 729 * N] x, y, z of the 9^3 corner points per block */
+  float *rho;          /* [512 * N]                                             */
+  float *vel;          /* [3 * 512 * N] ux, uy, uz per cell                     */
+  float *vel_mag;      /* [512 * N]                                             */
+  uint8_t *obstacle;   /* [512 * N] 0 / 1                                        */
+  int32_t *level;      /* [512 * N] level id                                     */
+  float *temperature;  /* [512 * N] (0 on levels without temperature)           */
+} ol_output_fields;
+
+/* Device part of export_merged_mesh_sync (io_vtk.jl:6-129): gathers the
+ * exported blocks of up to 16 levels into the packed arrays, NaN / +-Inf
+ * replaced by 0 (io_vtk.jl:111-115), velocity magnitude in Float32.  One
+ * launch on `stream`, asynchronous; the caller copies the arrays back and
+ * writes the file. */
+OL_API int ol_pack_merged_fields(const ol_output_level *levels, int32_t n_levels,
+                          const ol_output_fields *out, void *stream);
+
 /* Flow statistics of a level in FP64 (diagnostics.jl:43-93):
  * out[0..6] = {n_fluid, rho_sum, rho_min, rho_max, v_max, kinetic_energy,
  * mass_all_cells}.  `partials` >= ol_flow_stats_scratch_doubles(nB). */

@@ -92,6 +92,17 @@ class NetForceMaps(C.Structure):
                 ("net_fx", vp), ("net_fy", vp), ("net_fz", vp)]
 
 
+class OutputLevel(C.Structure):
+    _fields_ = [("rho", vp), ("vel", vp), ("obstacle", vp), ("temperature", vp), ("map_x", vp),
+                ("map_y", vp), ("map_z", vp), ("blocks", vp), ("n_export", i32),
+                ("n_blocks", i32), ("level_id", i32), ("dx", f32)]
+
+
+class OutputFields(C.Structure):
+    _fields_ = [("points", vp), ("rho", vp), ("vel", vp), ("vel_mag", vp), ("obstacle", vp),
+                ("level", vp), ("temperature", vp)]
+
+
 class ForceParams(C.Structure):
     _fields_ = [("dx", f32), ("dim_x", i32), ("dim_y", i32), ("dim_z", i32),
                 ("offset_x", f32), ("offset_y", f32), ("offset_z", f32),
@@ -152,6 +163,7 @@ _SIGS = {
     "ol_flow_stats": (C.c_int, [vp, vp, vp, i32, vp, C.POINTER(C.c_double), vp]),
     "ol_flow_stats_scratch_doubles": (C.c_size_t, [i32]),
     "ol_flow_stats_device": (C.c_int, [vp, vp, vp, i32, vp, vp, vp]),
+    "ol_pack_merged_fields": (C.c_int, [C.POINTER(OutputLevel), i32, C.POINTER(OutputFields), vp]),
     "ol_ghost_floats": (C.c_int64, [i32]),
     "ol_ctx_create": (C.c_int, [C.POINTER(vp), C.c_int, C.c_size_t, C.c_int]),
     "ol_ctx_destroy": (C.c_int, [vp]),

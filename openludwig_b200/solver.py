@@ -548,17 +548,34 @@ class Simulation:
         return self._coeff(raw, self.p.rho_physical, self.p.u_physical, self.p.reference_area,
                            self.p.reference_chord, self.cfg.symmetric_analysis), raw
 
-    def run(self, steps: int, diag_freq: int | None = None) -> list[dict]:
+    def run(self, steps: int, diag_freq: int | None = None,
+            output_dir: str | None = None) -> list[dict]:
+        """With output_dir, the merged flow field is exported every
+        cfg.output_freq steps (main.jl:259-263, io_vtk.jl) as
+        flow_%06d.vtu: gathered on the device at the batch end that crosses
+        the output step, copied back while the next batches run, and written
+        at the next output or at the end of run()."""
         cfg = self.cfg
         diag = diag_freq or cfg.diag_freq
         batch = max(1, cfg.async_depth)
         end = self.t + steps
         t = self.t + 1
+        pending = None
+        if output_dir is not None and getattr(self, "_out", None) is None:
+            from .output import MergedOutput
+            self._out = MergedOutput(self.levels)
         while t <= end:
             batch_end = min(t + batch - 1, end)
             actual = batch_end - t + 1
             u = ramp_velocity(cfg.u_target, batch_end, cfg.ramp_steps)
             execute_timestep_batch(self.levels, self.settings, t, actual, u, self.dims)
+            of = max(1, cfg.output_freq)
+            if output_dir is not None and batch_end % of < actual:
+                out_step = (batch_end // of) * of
+                if t <= out_step <= batch_end:
+                    if pending is not None:
+                        self._write(output_dir, pending)
+                    pending = self._out.pack(out_step)
             if batch_end % diag < actual or batch_end == end:
                 d = (batch_end // diag) * diag
                 if t <= d <= batch_end:
@@ -572,7 +589,16 @@ class Simulation:
                     self.history.append(rec)
             t = batch_end + 1
         self.t = end
+        if pending is not None:
+            self._write(output_dir, pending)
         return self.history
+
+    @staticmethod
+    def _write(output_dir: str, snap) -> None:
+        import os
+        from .output import write_vtu
+        os.makedirs(output_dir, exist_ok=True)
+        write_vtu(os.path.join(output_dir, "flow_%06d.vtu" % snap.t_step), snap.wait())
 
     def averaged(self):
         """print_averaged_summary (surface.jl:58-139) coefficients."""

@@ -84,6 +84,16 @@ def sphere_ddf():
     return c, mesh
 
 
+def build_case(workload: str):
+    """(cfg, mesh, domain params, host levels) of a named benchmark workload."""
+    from . import domain, scaling
+    makers = {"cube_3lvl": cube_3lvl, "sphere_1lvl": sphere_1lvl, "sphere_ddf": sphere_ddf}
+    cfg, mesh = makers[workload]()
+    p = scaling.compute_domain_from_mesh(cfg, mesh.min_bounds, mesh.max_bounds)
+    hosts = domain.setup_multilevel_domain(cfg, mesh, p)
+    return cfg, mesh, p, hosts
+
+
 @dc.dataclass
 class MixCase:
     kind: str

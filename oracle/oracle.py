@@ -2,8 +2,9 @@
 
 TEST INFRASTRUCTURE: imported only by tests/, __graft_entry__.smoke() and the
 CPU-baseline leg of bench.py.  The oracle restates the reference's Julia
-algorithm for the LBM time step and its host preprocessing (see the headers
-of ol_oracle_kernels.cpp and ol_oracle_domain.cpp); parity against the
+algorithm for the LBM time step, its host preprocessing, the surface forces
+and the merged flow output (see the headers of ol_oracle_kernels.cpp and
+ol_oracle_domain.cpp, and merged_output below); parity against the
 reference itself is unpinned because the reference ships no tests, golden
 vectors or fixtures and its Julia toolchain is absent here.
 """
@@ -230,6 +231,72 @@ def surface_net_forces(mesh_arrays, rho, vel, obstacle, block_ptr, n_blocks, fp_
                                  _p(obstacle), _p(block_ptr), C.c_int32(n_blocks), C.byref(fp),
                                  C.c_int32(1 if closed_body else 0), _p(maps), _p(net))
     return maps, net
+
+
+def merged_output(levels: list, t_step: int) -> dict:
+    """export_merged_mesh_sync (io_vtk.jl:6-129) restated with numpy loops
+    over blocks: levels = [dict(coords [n,3] 1-based, rho, vel, vel_temp,
+    obstacle, temperature or None, dx, level_id)], all flat Float32 / UInt8
+    host arrays in the reference layout.  Returns the arrays the reference
+    hands to vtk_grid (points [P,3], rho, vel [C,3], vel_mag, obstacle, level,
+    temperature when any level has one)."""
+    bs = 8
+    valid = []
+    for lvl, L in enumerate(levels):                                 # io_vtk.jl:19-38
+        nxt = None
+        if lvl + 1 < len(levels):
+            nxt = {tuple(int(v) for v in c) for c in levels[lvl + 1]["coords"]}
+        for b, (bx, by, bz) in enumerate(L["coords"]):
+            bx, by, bz = int(bx), int(by), int(bz)
+            export = True
+            if nxt is not None:
+                children = 0
+                for dbz in (0, 1):
+                    for dby in (0, 1):
+                        for dbx in (0, 1):
+                            if (2 * bx - 1 + dbx, 2 * by - 1 + dby, 2 * bz - 1 + dbz) in nxt:
+                                children += 1
+                export = children != 8
+            if export:
+                valid.append((lvl, b, bx, by, bz))
+    n = len(valid)
+    ddf = any(L.get("temperature") is not None for L in levels)
+    pts = np.empty((n * 729, 3), np.float32)
+    rho = np.empty(n * 512, np.float32)
+    vel = np.empty((n * 512, 3), np.float32)
+    obs = np.empty(n * 512, np.uint8)
+    lev = np.empty(n * 512, np.int32)
+    temp = np.zeros(n * 512, np.float32) if ddf else None
+    px, py, pz = np.meshgrid(np.arange(9), np.arange(9), np.arange(9), indexing="ij")
+    px, py, pz = px.T.reshape(-1), py.T.reshape(-1), pz.T.reshape(-1)   # x fastest
+    for i, (lvl, b, bx, by, bz) in enumerate(valid):                 # io_vtk.jl:68-107
+        L = levels[lvl]
+        dx = np.float32(L["dx"])
+        S = L["rho"].shape[0]
+        v = L["vel_temp"] if t_step % 2 == 0 else L["vel"]
+        o = np.float32((bx - 1) * 8), np.float32((by - 1) * 8), np.float32((bz - 1) * 8)
+        sl = slice(i * 729, (i + 1) * 729)
+        pts[sl, 0] = (o[0] + px.astype(np.float32)) * dx
+        pts[sl, 1] = (o[1] + py.astype(np.float32)) * dx
+        pts[sl, 2] = (o[2] + pz.astype(np.float32)) * dx
+        c = slice(i * 512, (i + 1) * 512)
+        src = slice(b * 512, (b + 1) * 512)
+        rho[c] = L["rho"][src]
+        vel[c, 0] = v[src]
+        vel[c, 1] = v[S + b * 512:S + (b + 1) * 512]
+        vel[c, 2] = v[2 * S + b * 512:2 * S + (b + 1) * 512]
+        obs[c] = (L["obstacle"][src] != 0).astype(np.uint8)
+        lev[c] = L["level_id"]
+        if ddf and L.get("temperature") is not None:
+            temp[c] = L["temperature"][src]
+    for a in (rho, vel, temp):                                       # io_vtk.jl:111-115
+        if a is not None:
+            a[~np.isfinite(a)] = 0.0
+    vmag = np.sqrt(vel[:, 0] * vel[:, 0] + vel[:, 1] * vel[:, 1] + vel[:, 2] * vel[:, 2])
+    out = dict(points=pts, rho=rho, vel=vel, vel_mag=vmag, obstacle=obs, level=lev)
+    if ddf:
+        out["temperature"] = temp
+    return out
 
 
 def double_to_half_bits(x: float) -> int:
