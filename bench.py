@@ -16,7 +16,7 @@ Reported:
   value       MLUPS (true cell updates / s, whole job) with the state resident
               in HBM; each coarse step replayed from a CUDA graph
   e2e         the same metric through the reference-facing C ABI, one
-              ol_stream_collide / ol_bouzidi_sparse call per level sub-step
+              ol_stream_collide / ol_bouzidi_apply_links call per level sub-step
               from the host driver, with the per-step diagnostic (FP64 flow
               statistics) read back to pinned host memory every step
   roofline    HBM roofline of the dominant kernel (finest-level stream-collide)

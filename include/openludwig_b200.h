@@ -164,6 +164,34 @@ OL_API int ol_bouzidi_sparse(float *f_out, const uint16_t *q_map,
                       int32_t n_blocks, float q_min_threshold, float *scratch,
                       void *stream);
 
+/* A boundary link of the Bouzidi correction: level-local cell index
+ * (b*512 + x + 8y + 64z, 0-based), q, direction k, and the cell x - c_k that
+ * q < 1/2 reads (-1: absent neighbour block, or q >= 1/2). */
+typedef struct ol_bouzidi_link {
+  int32_t cell;
+  int32_t far_cell;
+  float q;
+  int32_t k;
+} ol_bouzidi_link;
+
+/* Compacts the links of a level with q in (q_min, 1] (static for a level:
+ * build once) into `links` (capacity 27 * n_boundary) and their number into
+ * the device int *n_links_dev; arguments as ol_bouzidi_sparse.  No
+ * reference counterpart: ol_bouzidi_apply_links then corrects only those
+ * links each step instead of visiting all 27 directions of every boundary
+ * cell. */
+OL_API int ol_bouzidi_build_links(const uint16_t *q_map, const int32_t *cell_block,
+                           const int8_t *cell_x, const int8_t *cell_y,
+                           const int8_t *cell_z, int32_t n_boundary,
+                           const int32_t *neighbor_table, int32_t n_blocks,
+                           float q_min_threshold, ol_bouzidi_link *links,
+                           int32_t *n_links_dev, void *stream);
+/* The correction of ol_bouzidi_sparse (bouzidi_kernel.jl:13-92) over a link
+ * list: every corrected value gathered into scratch (n_links floats), then
+ * scattered.  The same values, bit for bit. */
+OL_API int ol_bouzidi_apply_links(float *f_out, const ol_bouzidi_link *links, int32_t n_links,
+                           int32_t n_blocks, float *scratch, void *stream);
+
 /* Same correction as ol_bouzidi_sparse for callers that cannot allocate
  * device memory: callers whose memory is held by another allocator's pool
  * (CUDA.jl, PyTorch caching allocators) or loops that must not allocate.

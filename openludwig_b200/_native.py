@@ -92,6 +92,10 @@ class NetForceMaps(C.Structure):
                 ("net_fx", vp), ("net_fy", vp), ("net_fz", vp)]
 
 
+class BouzidiLink(C.Structure):
+    _fields_ = [("cell", i32), ("far_cell", i32), ("q", f32), ("k", i32)]
+
+
 class OutputLevel(C.Structure):
     _fields_ = [("rho", vp), ("vel", vp), ("obstacle", vp), ("temperature", vp), ("map_x", vp),
                 ("map_y", vp), ("map_z", vp), ("blocks", vp), ("n_export", i32),
@@ -146,6 +150,8 @@ _SIGS = {
     "ol_bouzidi": (C.c_int, [vp, vp, vp, vp, vp, vp, vp, i32, vp, i32, f32, vp]),
     "ol_bouzidi_sparse": (C.c_int, [vp, vp, vp, vp, vp, vp, i32, vp, i32, f32, vp, vp]),
     "ol_bouzidi_sparse_noalloc": (C.c_int, [vp, vp, vp, vp, vp, vp, i32, vp, i32, f32, vp]),
+    "ol_bouzidi_build_links": (C.c_int, [vp, vp, vp, vp, vp, i32, vp, i32, f32, vp, vp, vp]),
+    "ol_bouzidi_apply_links": (C.c_int, [vp, vp, i32, i32, vp, vp]),
     "ol_thermal": (C.c_int, [C.POINTER(ThermalView), C.POINTER(ThermalParams), vp]),
     "ol_restrict": (C.c_int, [C.POINTER(RestrictView), vp]),
     "ol_voxelize": (C.c_int, [vp, i32, vp, i32, vp, vp, C.c_double, C.POINTER(C.c_double), vp,

@@ -34,6 +34,19 @@ __device__ __forceinline__ float half_bits_to_float(uint16_t h) {
   return __half2float(__ushort_as_half(h));
 }
 
+// The corrected value from the link's own post-collision f_k and, for
+// q < 1/2, f_k of the cell one link further in (fff), else f_opp(k) of the
+// cell itself (bouzidi_kernel.jl:60-87).
+__device__ __forceinline__ float bouzidi_value(float q, float fk, float fother) {
+  if (q < 0.5f) {
+    const float c1 = 2.0f * q;
+    return c1 * fk + (1.0f - c1) * fother;
+  }
+  const float inv2q = 1.0f / (2.0f * q);
+  const float c2 = (2.0f * q - 1.0f) * inv2q;
+  return inv2q * fk + c2 * fother;
+}
+
 template <class ST>
 __device__ __forceinline__ bool bouzidi_link(const BouzDev &B, int64_t i, int k, size_t &own,
                                              float &val) {
@@ -66,15 +79,54 @@ __device__ __forceinline__ bool bouzidi_link(const BouzDev &B, int64_t i, int k,
                                 BS * (ny & 7) + BS * BS * (nz & 7) + (size_t)k * B.dstride,
                        k, B.inv_scale);
     }
-    const float c1 = 2.0f * q;
-    val = c1 * fk + (1.0f - c1) * fff;
+    val = bouzidi_value(q, fk, fff);
   } else {
-    const float fo = ST::load(src, own + (size_t)ko * B.dstride, ko, B.inv_scale);
-    const float inv2q = 1.0f / (2.0f * q);
-    const float c2 = (2.0f * q - 1.0f) * inv2q;
-    val = inv2q * fk + c2 * fo;
+    val = bouzidi_value(q, fk, ST::load(src, own + (size_t)ko * B.dstride, ko, B.inv_scale));
   }
   return true;
+}
+
+// ---------------------------------------------------------------------------
+// Link lists: the (cell, direction) pairs whose q lies in (q_min, 1] are
+// static for a level, so they are compacted once (k_bouzidi_build_links)
+// and each step touches only them: a gather over the links into scratch,
+// then a scatter, with the same arithmetic as above.  Cells are level-local
+// (block_offset * 512 is added when the list is applied); far_cell is the
+// cell x - c_k for q < 1/2, -1 when that neighbour block is absent (the
+// value then falls back to f_k) or when q >= 1/2.
+// ---------------------------------------------------------------------------
+template <class ST>
+__global__ void k_bouzidi_links_gather(const void *f_v, const ol_bouzidi_link *__restrict__ links,
+                                       int32_t n_links, int64_t cell0, int64_t dstride,
+                                       float inv_scale, float *__restrict__ scratch) {
+  const int l = blockIdx.x * blockDim.x + threadIdx.x;
+  if (l >= n_links) return;
+  using T = typename ST::T;
+  const T *f = (const T *)f_v;
+  const ol_bouzidi_link L = links[l];
+  const int k = L.k;
+  const size_t own = (size_t)(cell0 + L.cell);
+  const float fk = ST::load(f, own + (size_t)k * dstride, k, inv_scale);
+  float fother;
+  if (L.q < 0.5f)
+    fother = L.far_cell >= 0 ? ST::load(f, (size_t)(cell0 + L.far_cell) + (size_t)k * dstride, k,
+                                        inv_scale)
+                             : fk;
+  else
+    fother = ST::load(f, own + (size_t)opp_of(k) * dstride, opp_of(k), inv_scale);
+  scratch[l] = bouzidi_value(L.q, fk, fother);
+}
+
+template <class ST>
+__global__ void k_bouzidi_links_scatter(void *f_v, const ol_bouzidi_link *__restrict__ links,
+                                        int32_t n_links, int64_t cell0, int64_t dstride,
+                                        float scale, const float *__restrict__ scratch) {
+  const int l = blockIdx.x * blockDim.x + threadIdx.x;
+  if (l >= n_links) return;
+  const ol_bouzidi_link L = links[l];
+  const int ko = opp_of(L.k);
+  ST::store((typename ST::T *)f_v, (size_t)(cell0 + L.cell) + (size_t)ko * dstride, ko, scale,
+            scratch[l]);
 }
 
 // Single phase: src != f (reference semantics with a post-collision copy).

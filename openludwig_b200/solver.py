@@ -16,7 +16,8 @@ Differences from the reference that do not change results:
     untouched, so f_old / vel_old alias f_in / vel_in and only rho (which the
     step overwrites in place) is copied.
   * Bouzidi runs in the sparse two-phase form (gather corrected links, then
-    scatter) so the dense post-collision copy f_post is never written.
+    scatter) over the level's static list of cut links, so the dense
+    post-collision copy f_post is never written.
 """
 from __future__ import annotations
 
@@ -79,6 +80,9 @@ class DeviceLevel:
     # list ends with one unused entry
     ghost_list: torch.Tensor | None = None
     edge_list: torch.Tensor | None = None
+    # Bouzidi links (cells x directions with q in (q_min, 1]), built once
+    bz_links: torch.Tensor | None = None
+    bz_n_links: int = 0
     # thermal DDF
     g: torch.Tensor | None = None
     g_temp: torch.Tensor | None = None
@@ -326,9 +330,10 @@ def perform_timestep(s: StepSettings, lv: DeviceLevel, parent: ParentRef | None,
                    _ptr(lv.cell_x), _ptr(lv.cell_y), _ptr(lv.cell_z), N.i32(h.n_boundary),
                    _ptr(lv.neighbor_table), N.i32(n), N.f32(s.q_min), st)
         else:
-            N.call("ol_bouzidi_sparse", _ptr(f_out), _ptr(lv.q_map), _ptr(lv.cell_block),
-                   _ptr(lv.cell_x), _ptr(lv.cell_y), _ptr(lv.cell_z), N.i32(h.n_boundary),
-                   _ptr(lv.neighbor_table), N.i32(n), N.f32(s.q_min), _ptr(lv.bouzidi_scratch), st)
+            if lv.bz_links is None:
+                build_bouzidi_links(lv, s.q_min)
+            N.call("ol_bouzidi_apply_links", _ptr(f_out), _ptr(lv.bz_links),
+                   N.i32(lv.bz_n_links), N.i32(n), _ptr(lv.bouzidi_scratch), st)
     if s.ddf and g_out is not None:
         tp = N.ThermalParams(tau_g=lv.host.tau_g, tau_g_parent=parent.lv.host.tau_g if parent else 0.5,
                              is_level_1=int(is_l1), is_symmetric=s.is_symmetric,
@@ -353,10 +358,10 @@ def perform_timestep(s: StepSettings, lv: DeviceLevel, parent: ParentRef | None,
             tv.p_n_blocks = p.n_blocks
         N.call("ol_thermal", C.byref(tv), C.byref(tp), st)
         if lv.has_bouzidi:
-            h = lv.host
-            N.call("ol_bouzidi_sparse", _ptr(g_out), _ptr(lv.q_map), _ptr(lv.cell_block),
-                   _ptr(lv.cell_x), _ptr(lv.cell_y), _ptr(lv.cell_z), N.i32(h.n_boundary),
-                   _ptr(lv.neighbor_table), N.i32(n), N.f32(s.q_min), _ptr(lv.bouzidi_scratch), st)
+            if lv.bz_links is None:
+                build_bouzidi_links(lv, s.q_min)
+            N.call("ol_bouzidi_apply_links", _ptr(g_out), _ptr(lv.bz_links),
+                   N.i32(lv.bz_n_links), N.i32(n), _ptr(lv.bouzidi_scratch), st)
 
 
 def recursive_step(levels: list, s: StepSettings, lvl: int, t_sub: int, parent: ParentRef | None,
@@ -393,6 +398,19 @@ def recursive_step(levels: list, s: StepSettings, lvl: int, t_sub: int, parent: 
         if s.restriction:
             # the child's second sub-step (odd t_sub) wrote f and vel
             restrict_level(levels[lvl + 1], me, s)
+
+
+def build_bouzidi_links(lv: DeviceLevel, q_min: float) -> None:
+    """The level's Bouzidi link list (ol_bouzidi_build_links): static, built
+    on first use; the correction then visits only those links."""
+    h = lv.host
+    links = torch.empty((27 * h.n_boundary + 1) * 4, dtype=torch.int32, device=lv.f.device)
+    count = torch.zeros(1, dtype=torch.int32, device=lv.f.device)
+    N.call("ol_bouzidi_build_links", _ptr(lv.q_map), _ptr(lv.cell_block), _ptr(lv.cell_x),
+           _ptr(lv.cell_y), _ptr(lv.cell_z), N.i32(h.n_boundary), _ptr(lv.neighbor_table),
+           N.i32(lv.n_blocks), N.f32(q_min), _ptr(links), _ptr(count), _stream())
+    lv.bz_n_links = int(count.item())
+    lv.bz_links = links
 
 
 def restrict_level(child: DeviceLevel, parent: ParentRef, s: StepSettings) -> None:

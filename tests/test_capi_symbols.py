@@ -71,7 +71,7 @@ def test_ctypes_struct_layouts_match_header(tmp_path):
              "ol_parent_view": N.ParentView, "ol_thermal_view": N.ThermalView,
              "ol_surface_mesh": N.SurfaceMesh, "ol_restrict_view": N.RestrictView,
              "ol_net_force_maps": N.NetForceMaps, "ol_output_level": N.OutputLevel,
-             "ol_output_fields": N.OutputFields}
+             "ol_output_fields": N.OutputFields, "ol_bouzidi_link": N.BouzidiLink}
     src = tmp_path / "sizes.c"
     src.write_text('#include <stdio.h>\n#include "openludwig_b200.h"\nint main(void){\n' +
                    "".join(f'printf("%zu\\n", sizeof({n}));\n' for n in names) + "return 0;}\n")

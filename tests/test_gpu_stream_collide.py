@@ -283,3 +283,27 @@ def test_two_level_thermal_ddf():
         assert rel_err(lg.f_temp.cpu().numpy(), lo.f_temp) < 1e-4
         assert rel_err(lg.g_temp.cpu().numpy(), lo.g_temp) < 1e-4
         assert rel_err(lg.temperature.cpu().numpy(), lo.T) < 1e-5
+
+
+def test_bouzidi_links_equal_sparse_form(case1):
+    """The link-list correction (ol_bouzidi_build_links + _apply_links) gives
+    the bits of ol_bouzidi_sparse, which visits every direction of every
+    boundary cell."""
+    c, mesh, p, hosts = case1
+    h = hosts[0]
+    n = h.n_blocks
+    rng = np.random.default_rng(8)
+    f0 = (np.repeat(weights32(), 512 * n) * rng.uniform(0.9, 1.1, 27 * 512 * n)).astype(np.float32)
+    lv = S.upload_level(h, DEV)
+    a, b = _t(f0), _t(f0)
+    st = S.StepSettings.from_config(c, False)
+    N.call("ol_bouzidi_sparse", S._ptr(a), S._ptr(lv.q_map), S._ptr(lv.cell_block),
+           S._ptr(lv.cell_x), S._ptr(lv.cell_y), S._ptr(lv.cell_z), N.i32(h.n_boundary),
+           S._ptr(lv.neighbor_table), N.i32(n), N.f32(st.q_min), S._ptr(lv.bouzidi_scratch),
+           S._stream())
+    S.build_bouzidi_links(lv, st.q_min)
+    assert 0 < lv.bz_n_links < 27 * h.n_boundary
+    N.call("ol_bouzidi_apply_links", S._ptr(b), S._ptr(lv.bz_links), N.i32(lv.bz_n_links),
+           N.i32(n), S._ptr(lv.bouzidi_scratch), S._stream())
+    torch.cuda.synchronize()
+    assert torch.equal(a, b) and not torch.equal(a, _t(f0))
