@@ -53,9 +53,10 @@ __global__ void __launch_bounds__(512, 2)
 // Batched Bouzidi: one thread per (boundary cell, direction) over the
 // concatenated boundary lists of a slot; `f_of_desc` selects f_out (flow)
 // or g_out (thermal) of the owning descriptor.
-struct BouzItem {
-  int32_t bdesc;   // index into BouzDev array
-  int32_t cell;    // boundary-cell index within that list
+// One cut link of a batched Bouzidi list: its level list and index there.
+struct BouzLinkItem {
+  int32_t bdesc;
+  int32_t link;
 };
 
 }  // namespace ol

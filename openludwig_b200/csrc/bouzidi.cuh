@@ -28,6 +28,7 @@ struct BouzDev {
   int32_t desc;         // batched: owning level descriptor (f = its f_out / g_out)
   int32_t thermal;      // batched: correct the thermal populations instead
   int64_t scratch_off;  // batched: first scratch slot of this list
+  const ol_bouzidi_link *links;  // batched: the level's cut links (level-local cells)
 };
 
 __device__ __forceinline__ float half_bits_to_float(uint16_t h) {

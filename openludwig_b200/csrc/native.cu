@@ -169,43 +169,49 @@ __global__ void __launch_bounds__(512, OP == OL_OP_CUMULANT ? 2 : 1)
   }
 }
 
+// Bouzidi for the Bouzidi lists of many cases over their static lists of cut
+// links (built at case admission): one thread per link, the corrected
+// values gathered into scratch, then scattered (the arithmetic of
+// bouzidi_value, as the drop-in link kernels).
 template <class ST>
-__global__ void k_bouz_gather_b(const LevelDev *descs, const ThermalDev *tdescs,
-                                const BouzDev *bd, const BouzItem *items, int64_t n_links,
-                                float *scratch) {
+__global__ void k_bouz_links_gather_b(const LevelDev *descs, const ThermalDev *tdescs,
+                                      const BouzDev *bd, const BouzLinkItem *items, int64_t n,
+                                      float *scratch) {
   const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (j >= n_links) return;
-  const int64_t n_items = n_links / 27;  // direction-major: neighbouring threads
-  const int k = (int)(j / n_items);        // take neighbouring boundary cells
-  const BouzItem it = items[j - (int64_t)k * n_items];
-  BouzDev B = bd[it.bdesc];
-  void *f = B.thermal ? tdescs[B.desc].g_out : descs[B.desc].f_out;
-  B.f = f;
-  B.src = f;
-  size_t own;
-  float v;
-  if (bouzidi_link<ST>(B, it.cell, k, own, v)) scratch[B.scratch_off + (int64_t)it.cell * 27 + k] = v;
+  if (j >= n) return;
+  const BouzLinkItem it = items[j];
+  const BouzDev &B = bd[it.bdesc];
+  using T = typename ST::T;
+  const T *f = (const T *)(B.thermal ? tdescs[B.desc].g_out : descs[B.desc].f_out);
+  const ol_bouzidi_link L = B.links[it.link];
+  const int k = L.k;
+  const size_t cell0 = (size_t)B.block_offset * BCELLS;
+  const size_t own = cell0 + (size_t)L.cell;
+  const float fk = ST::load(f, own + (size_t)k * B.dstride, k, B.inv_scale);
+  float fother;
+  if (L.q < 0.5f)
+    fother = L.far_cell >= 0
+                 ? ST::load(f, cell0 + (size_t)L.far_cell + (size_t)k * B.dstride, k, B.inv_scale)
+                 : fk;
+  else
+    fother = ST::load(f, own + (size_t)opp_of(k) * B.dstride, opp_of(k), B.inv_scale);
+  scratch[B.scratch_off + it.link] = bouzidi_value(L.q, fk, fother);
 }
 
 template <class ST>
-__global__ void k_bouz_scatter_b(const LevelDev *descs, const ThermalDev *tdescs,
-                                 const BouzDev *bd, const BouzItem *items, int64_t n_links,
-                                 const float *scratch) {
+__global__ void k_bouz_links_scatter_b(const LevelDev *descs, const ThermalDev *tdescs,
+                                       const BouzDev *bd, const BouzLinkItem *items, int64_t n,
+                                       const float *scratch) {
   const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (j >= n_links) return;
-  const int64_t n_items = n_links / 27;  // direction-major: neighbouring threads
-  const int k = (int)(j / n_items);        // take neighbouring boundary cells
-  const BouzItem it = items[j - (int64_t)k * n_items];
+  if (j >= n) return;
+  const BouzLinkItem it = items[j];
   const BouzDev &B = bd[it.bdesc];
   void *f = B.thermal ? tdescs[B.desc].g_out : descs[B.desc].f_out;
-  const int i = it.cell;
-  const int b = B.cell_block[i] - 1;
-  const int x = B.cell_x[i] - 1, y = B.cell_y[i] - 1, z = B.cell_z[i] - 1;
-  const size_t own = (size_t)(B.block_offset + b) * BCELLS + x + BS * y + BS * BS * z;
-  const float q = half_bits_to_float(B.q[(int64_t)i * 27 + k]);
-  if (!(q > B.q_min && q <= 1.0f)) return;
-  ST::store((typename ST::T *)f, own + (size_t)opp_of(k) * B.dstride, opp_of(k), B.scale,
-            scratch[B.scratch_off + (int64_t)i * 27 + k]);
+  const ol_bouzidi_link L = B.links[it.link];
+  const int ko = opp_of(L.k);
+  ST::store((typename ST::T *)f, (size_t)B.block_offset * BCELLS + (size_t)L.cell +
+                                     (size_t)ko * B.dstride,
+            ko, B.scale, scratch[B.scratch_off + it.link]);
 }
 
 // Initial state of a pool region (main.jl:113-150): f = w (shifted FP16: 0),
@@ -255,6 +261,8 @@ struct DevLevel {
   int32_t dims[3] = {0, 0, 0};
   int32_t n_boundary = 0;
   uint16_t *q = nullptr;
+  ol_bouzidi_link *links = nullptr;  // cut links, level-local cells
+  int32_t n_links = 0;
   int32_t *cb = nullptr;
   int8_t *cx = nullptr, *cy = nullptr, *cz = nullptr;
   float tau = 0.5f, tau_g = 0.5f, scale = 1.0f;
@@ -355,7 +363,7 @@ struct ol_ctx {
   ol::DescMeta *d_meta = nullptr;
   ol::WorkItem *d_items = nullptr;
   ol::BouzDev *d_bdescs = nullptr;
-  ol::BouzItem *d_bitems = nullptr;
+  ol::BouzLinkItem *d_blitems = nullptr;
   float *d_bscratch = nullptr;
   int n_desc = 0;
   std::vector<ol::Launch> plan;
@@ -379,12 +387,60 @@ static size_t per_block_bytes(bool f16, bool ddf) {
   return b;
 }
 
+// IEEE binary16 bits -> float on the host (exact; the q-map holds binary16).
+static float half_bits_to_float_host(uint16_t h) {
+  const int e = (h >> 10) & 31, m = h & 1023;
+  float v;
+  if (e == 0) v = std::ldexp((float)m, -24);
+  else if (e == 31) v = m ? NAN : INFINITY;
+  else v = std::ldexp((float)(m | 1024), e - 25);
+  return (h & 0x8000) ? -v : v;
+}
+
+// The level's cut links (q in (q_min, 1]) in direction-major order, as
+// k_bouzidi_build_links builds them on the device for the drop-in path.
+static std::vector<ol_bouzidi_link> cut_links(const ol_level_desc &S, float q_min) {
+  std::vector<ol_bouzidi_link> out;
+  const size_t Sd = (size_t)S.n_blocks * BCELLS;
+  for (int k = 0; k < 27; ++k)
+    for (int i = 0; i < S.n_boundary; ++i) {
+      const int b = S.cell_block[i] - 1;
+      const int x = S.cell_x[i] - 1, y = S.cell_y[i] - 1, z = S.cell_z[i] - 1;
+      const int own = b * BCELLS + x + BS * y + BS * BS * z;
+      const uint16_t h = S.q_map[own + k * Sd];
+      // positive binary16 values order like their bits: skip 0, negatives,
+      // NaN and values above 1 (0x3C00) before converting
+      if (h == 0 || (h & 0x8000) || h > 0x3C00) continue;
+      const float q = half_bits_to_float_host(h);
+      if (!(q > q_min && q <= 1.0f)) continue;
+      ol_bouzidi_link L{own, -1, q, k};
+      if (q < 0.5f) {
+        const int nx = x - cx_of(k), ny = y - cy_of(k), nz = z - cz_of(k);
+        if (nx >= 0 && nx < BS && ny >= 0 && ny < BS && nz >= 0 && nz < BS) {
+          L.far_cell = b * BCELLS + nx + BS * ny + BS * BS * nz;
+        } else {
+          const int ox = nx < 0 ? -1 : (nx >= BS ? 1 : 0);
+          const int oy = ny < 0 ? -1 : (ny >= BS ? 1 : 0);
+          const int oz = nz < 0 ? -1 : (nz >= BS ? 1 : 0);
+          const int nb = S.neighbor_table[b + (size_t)S.n_blocks *
+                                                  ((ox + 1) + 3 * (oy + 1) + 9 * (oz + 1))];
+          if (nb > 0) L.far_cell = (nb - 1) * BCELLS + (nx & 7) + BS * (ny & 7) + BS * BS * (nz & 7);
+        }
+      }
+      out.push_back(L);
+    }
+  return out;
+}
+
 static size_t case_meta_bytes(const ol_case_desc *cd) {
   size_t b = 0;
   for (int l = 0; l < cd->n_levels; ++l) {
     const ol_level_desc &L = cd->levels[l];
     b += (size_t)L.n_blocks * (27 + 3) * 4 + (size_t)L.dim_x * L.dim_y * L.dim_z * 4;
     b += (size_t)L.n_boundary * (27 * 2 + 4 + 3);
+    if (L.n_boundary > 0)
+      b += cut_links(L, cd->q_min_threshold > 0.0f ? cd->q_min_threshold : 0.001f).size() *
+           sizeof(ol_bouzidi_link);
     if (l > 0)  // ghost rows of both sub-steps of a pair, flow (+ thermal)
       b += blocks_with_absent_neighbour(L).size() * kHaloEntries * sizeof(float) * 2 *
                (cd->ddf ? 2 : 1) +
@@ -435,6 +491,7 @@ static void free_case_meta(NCase &c) {
   for (auto &L : c.levels) {
     cudaFree(L.nbr); cudaFree(L.mx); cudaFree(L.my); cudaFree(L.mz); cudaFree(L.bptr);
     cudaFree(L.q); cudaFree(L.cb); cudaFree(L.cx); cudaFree(L.cy); cudaFree(L.cz);
+    cudaFree(L.links);
     cudaFree(L.ghost); cudaFree(L.ghost_g); cudaFree(L.ghost2); cudaFree(L.ghost_g2);
     cudaFree(L.gidx);
   }
@@ -446,9 +503,9 @@ static void free_plan(ol_ctx *c) {
   if (c->exec) cudaGraphExecDestroy(c->exec);
   c->exec = nullptr;
   cudaFree(c->d_descs); cudaFree(c->d_tdescs); cudaFree(c->d_meta); cudaFree(c->d_items);
-  cudaFree(c->d_bdescs); cudaFree(c->d_bitems); cudaFree(c->d_bscratch);
+  cudaFree(c->d_bdescs); cudaFree(c->d_blitems); cudaFree(c->d_bscratch);
   c->d_descs = nullptr; c->d_tdescs = nullptr; c->d_meta = nullptr; c->d_items = nullptr;
-  c->d_bdescs = nullptr; c->d_bitems = nullptr; c->d_bscratch = nullptr;
+  c->d_bdescs = nullptr; c->d_blitems = nullptr; c->d_bscratch = nullptr;
   c->plan.clear();
   c->n_desc = 0;
 }
@@ -507,13 +564,21 @@ static void record_step(ol_ctx *c) {
             c->d_descs, c->d_items + l.off);
     } else {
       const unsigned g = (unsigned)((l.n + 255) / 256);
-      const BouzItem *items = c->d_bitems + l.off / 27;
+      const BouzLinkItem *items = c->d_blitems + l.off;
       if (l.kind == 1) {
-        if (c->f16) k_bouz_gather_b<StoreF16S><<<g, 256, 0, c->stream>>>(c->d_descs, c->d_tdescs, c->d_bdescs, items, l.n, c->d_bscratch);
-        else k_bouz_gather_b<StoreF32><<<g, 256, 0, c->stream>>>(c->d_descs, c->d_tdescs, c->d_bdescs, items, l.n, c->d_bscratch);
+        if (c->f16)
+          k_bouz_links_gather_b<StoreF16S><<<g, 256, 0, c->stream>>>(
+              c->d_descs, c->d_tdescs, c->d_bdescs, items, l.n, c->d_bscratch);
+        else
+          k_bouz_links_gather_b<StoreF32><<<g, 256, 0, c->stream>>>(
+              c->d_descs, c->d_tdescs, c->d_bdescs, items, l.n, c->d_bscratch);
       } else {
-        if (c->f16) k_bouz_scatter_b<StoreF16S><<<g, 256, 0, c->stream>>>(c->d_descs, c->d_tdescs, c->d_bdescs, items, l.n, c->d_bscratch);
-        else k_bouz_scatter_b<StoreF32><<<g, 256, 0, c->stream>>>(c->d_descs, c->d_tdescs, c->d_bdescs, items, l.n, c->d_bscratch);
+        if (c->f16)
+          k_bouz_links_scatter_b<StoreF16S><<<g, 256, 0, c->stream>>>(
+              c->d_descs, c->d_tdescs, c->d_bdescs, items, l.n, c->d_bscratch);
+        else
+          k_bouz_links_scatter_b<StoreF32><<<g, 256, 0, c->stream>>>(
+              c->d_descs, c->d_tdescs, c->d_bdescs, items, l.n, c->d_bscratch);
       }
     }
   }
@@ -541,7 +606,8 @@ static int rebuild(ol_ctx *c) {
   std::vector<DescMeta> meta;
   std::vector<WorkItem> items;
   std::vector<BouzDev> bdescs;
-  std::vector<BouzItem> bitems;
+  std::vector<BouzLinkItem> blitems;  // one per cut link of the slot's lists
+  std::vector<int32_t> bcount;         // links of each Bouzidi list
   int64_t scratch_max = 0;
   const int64_t dstride = c->capacity * BCELLS;
   const uint32_t *tab = halo_table_device();
@@ -634,22 +700,25 @@ static int rebuild(ol_ctx *c) {
       meta.push_back(m);
       const int variant = cs.sp.op * 4 + (cs.sp.c_wale != 0.0f ? 2 : 0) + (cs.ddf ? 1 : 0);
       groups[variant].push_back(d);
-      if (V.n_boundary > 0) {
+      if (V.n_links > 0) {
         BouzDev B{};
         B.q = V.q; B.dense_q = 0; B.cell_block = V.cb; B.cell_x = V.cx; B.cell_y = V.cy;
         B.cell_z = V.cz; B.n_boundary = V.n_boundary; B.nbr = V.nbr; B.nbr_stride = V.n_blocks;
         B.block_offset = V.block_offset; B.dstride = dstride; B.q_min = cs.q_min;
         B.scale = V.scale; B.inv_scale = 1.0f / V.scale; B.desc = d; B.thermal = 0;
+        B.links = V.links;
         B.scratch_off = scratch_off;
-        scratch_off += (int64_t)V.n_boundary * 27;
+        scratch_off += V.n_links;
         bz_flow.push_back((int)bdescs.size());
         bdescs.push_back(B);
+        bcount.push_back(V.n_links);
         if (cs.ddf) {
           B.thermal = 1;
           B.scratch_off = scratch_off;
-          scratch_off += (int64_t)V.n_boundary * 27;
+          scratch_off += V.n_links;
           bz_therm.push_back((int)bdescs.size());
           bdescs.push_back(B);
+          bcount.push_back(V.n_links);
         }
       }
     }
@@ -684,11 +753,10 @@ static int rebuild(ol_ctx *c) {
     for (int pass = 0; pass < 2; ++pass) {
       const std::vector<int> &lst = pass == 0 ? bz_flow : bz_therm;
       if (lst.empty()) continue;
-      const int64_t first = (int64_t)bitems.size();
+      const int64_t first = (int64_t)blitems.size();
       for (int bi : lst)
-        for (int i = 0; i < bdescs[bi].n_boundary; ++i) bitems.push_back(BouzItem{bi, i});
-      const int64_t nl = ((int64_t)bitems.size() - first) * 27;
-      Launch g{}; g.kind = 1; g.off = first * 27; g.n = nl;
+        for (int l = 0; l < bcount[bi]; ++l) blitems.push_back(BouzLinkItem{bi, l});
+      Launch g{}; g.kind = 1; g.off = first; g.n = (int64_t)blitems.size() - first;
       Launch s2 = g; s2.kind = 2;
       c->plan.push_back(g);
       c->plan.push_back(s2);
@@ -703,7 +771,7 @@ static int rebuild(ol_ctx *c) {
   if ((rc = upload(&c->d_meta, meta.data(), meta.size()))) return rc;
   if ((rc = upload(&c->d_items, items.data(), items.size()))) return rc;
   if ((rc = upload(&c->d_bdescs, bdescs.data(), bdescs.size()))) return rc;
-  if ((rc = upload(&c->d_bitems, bitems.data(), bitems.size()))) return rc;
+  if ((rc = upload(&c->d_blitems, blitems.data(), blitems.size()))) return rc;
   if (scratch_max > 0) OL_CUDA(cudaMalloc(&c->d_bscratch, scratch_max * sizeof(float)));
   c->launches_per_step = per_step;
 
@@ -919,6 +987,10 @@ extern "C" int ol_ctx_case_add(ol_ctx *c, const ol_case_desc *cd, int32_t *case_
         for (int k = 0; k < 27; ++k) qs[(size_t)i * 27 + k] = S.q_map[own + k * Sd];
       }
       if ((rc = upload(&V.q, qs.data(), qs.size()))) return rc;
+      const std::vector<ol_bouzidi_link> links =
+          cut_links(S, cd->q_min_threshold > 0.0f ? cd->q_min_threshold : 0.001f);
+      V.n_links = (int32_t)links.size();
+      if (!links.empty() && (rc = upload(&V.links, links.data(), links.size()))) return rc;
       if ((rc = upload(&V.cb, S.cell_block, (size_t)S.n_boundary))) return rc;
       if ((rc = upload(&V.cx, S.cell_x, (size_t)S.n_boundary))) return rc;
       if ((rc = upload(&V.cy, S.cell_y, (size_t)S.n_boundary))) return rc;
