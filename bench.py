@@ -166,6 +166,26 @@ def build_case(workload: str):
         raise SystemExit(f"unknown workload {workload}")
 
 
+def launches_per_coarse_step(levels, ddf: bool) -> int:
+    """Kernels one coarse step launches through the drop-in path (after the
+    first step built the ghost visit lists and Bouzidi links): per level
+    sub-step one stream-collide and, with Bouzidi, a gather and a scatter;
+    on a refined level one ghost pass per pair of sub-steps, plus one for the
+    second sub-step when a block touches the domain boundary; the thermal
+    DDF repeats all of it for the temperature populations."""
+    total = 0
+    for i, lv in enumerate(levels):
+        n_sub = 1 << i
+        per = n_sub + (2 * n_sub if lv.has_bouzidi and lv.bz_n_links > 0 else 0)
+        if lv.ghost is not None:
+            if lv.ghost2 is None:
+                per += n_sub
+            else:
+                per += (n_sub // 2) * ((lv.ghost_list.numel() > 1) + (lv.edge_list.numel() > 1))
+        total += per * (2 if ddf else 1)
+    return total
+
+
 def describe(workload, p, hosts) -> dict:
     return {"workload": workload, "levels": len(hosts),
             "coarse_domain": [p.nx_coarse, p.ny_coarse, p.nz_coarse],
@@ -268,11 +288,6 @@ def main():
     upd = sum(h.n_blocks * 512 * (1 << i) for i, h in enumerate(hosts))
     # per level sub-step: [ghost pass] + stream-collide + Bouzidi gather/scatter,
     # and the same again for the thermal populations of a DDF case
-    per_sub = [1 + (lv.ghost is not None) + (2 if lv.has_bouzidi else 0) for lv in levels]
-    if cfg.ddf_enabled:
-        per_sub = [n + 1 + (lv.ghost_g is not None) + (2 if lv.has_bouzidi else 0)
-                   for n, lv in zip(per_sub, levels)]
-    launches_per_step = sum((1 << i) * n for i, n in enumerate(per_sub))
 
     stream = torch.cuda.Stream(device=dev)
     state = {"t": 0}
@@ -286,6 +301,8 @@ def main():
             state["t"] += 1
             coarse_step(state["t"])
     torch.cuda.synchronize()
+
+    launches_per_step = launches_per_coarse_step(levels, bool(cfg.ddf_enabled))
 
     # CUDA graph of two coarse steps (odd + even parity) for the device-resident run
     graph = torch.cuda.CUDAGraph()
@@ -352,7 +369,13 @@ def main():
     e2e_rate, e2e_ms = replicas.job_rate(upd * ke, ee0.elapsed_time(ee1), dev)
     e2e = e2e_rate / 1e6
     clocks = clk.stop()
-    h2d_per_step = launches_per_step * C.sizeof(N.StepParams)
+    # host-to-device bytes of a coarse step: what each C-ABI call passes by
+    # value (level view, parent view and step parameters per stream-collide;
+    # six pointer / scalar arguments per Bouzidi call; the flow statistics call)
+    sc_calls = sum(1 << i for i in range(len(levels)))
+    bz_calls = sum(1 << i for i, lv in enumerate(levels) if lv.has_bouzidi)
+    h2d_per_step = (sc_calls * (C.sizeof(N.LevelView) + C.sizeof(N.ParentView) +
+                                C.sizeof(N.StepParams)) + bz_calls * 6 * 8 + 7 * 8)
 
     # roofline of the dominant kernel: the finest level's ol_stream_collide
     # calls, timed as the pair of sub-steps a refined level takes per parent
