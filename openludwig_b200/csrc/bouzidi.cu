@@ -135,16 +135,18 @@ void launch_bouzidi_links(void *f, const ol_bouzidi_link *links, int32_t n_links
                           int64_t dstride, float scale, float *scratch, bool f16, cudaStream_t s) {
   if (n_links <= 0) return;
   const int grid = (n_links + 255) / 256;
+  const void *fc = f;
+  const float *sc = scratch;
   if (f16) {
-    k_bouzidi_links_gather<StoreF16S><<<grid, 256, 0, s>>>(f, links, n_links, cell0, dstride,
-                                                           1.0f / scale, scratch);
-    k_bouzidi_links_scatter<StoreF16S><<<grid, 256, 0, s>>>(f, links, n_links, cell0, dstride,
-                                                            scale, scratch);
+    launch_pdl(k_bouzidi_links_gather<StoreF16S>, grid, 256, 0, s, fc, links, n_links, cell0,
+               dstride, 1.0f / scale, scratch);
+    launch_pdl(k_bouzidi_links_scatter<StoreF16S>, grid, 256, 0, s, f, links, n_links, cell0,
+               dstride, scale, sc);
   } else {
-    k_bouzidi_links_gather<StoreF32><<<grid, 256, 0, s>>>(f, links, n_links, cell0, dstride, 1.0f,
-                                                          scratch);
-    k_bouzidi_links_scatter<StoreF32><<<grid, 256, 0, s>>>(f, links, n_links, cell0, dstride, 1.0f,
-                                                           scratch);
+    launch_pdl(k_bouzidi_links_gather<StoreF32>, grid, 256, 0, s, fc, links, n_links, cell0,
+               dstride, 1.0f, scratch);
+    launch_pdl(k_bouzidi_links_scatter<StoreF32>, grid, 256, 0, s, f, links, n_links, cell0,
+               dstride, 1.0f, sc);
   }
 }
 

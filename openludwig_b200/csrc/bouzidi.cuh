@@ -9,6 +9,7 @@
 // f*[x,k].  The written slot is post-collision / pre-stream, exactly as in
 // the reference.
 #pragma once
+#include "common.cuh"
 #include "level_dev.cuh"
 
 namespace ol {
@@ -100,6 +101,7 @@ template <class ST>
 __global__ void k_bouzidi_links_gather(const void *f_v, const ol_bouzidi_link *__restrict__ links,
                                        int32_t n_links, int64_t cell0, int64_t dstride,
                                        float inv_scale, float *__restrict__ scratch) {
+  pdl_wait();  // f: written by the stream-collide launch before
   const int l = blockIdx.x * blockDim.x + threadIdx.x;
   if (l >= n_links) return;
   using T = typename ST::T;
@@ -122,6 +124,7 @@ template <class ST>
 __global__ void k_bouzidi_links_scatter(void *f_v, const ol_bouzidi_link *__restrict__ links,
                                         int32_t n_links, int64_t cell0, int64_t dstride,
                                         float scale, const float *__restrict__ scratch) {
+  pdl_wait();  // scratch: filled by the gather launch before
   const int l = blockIdx.x * blockDim.x + threadIdx.x;
   if (l >= n_links) return;
   const ol_bouzidi_link L = links[l];

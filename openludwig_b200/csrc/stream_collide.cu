@@ -75,6 +75,7 @@ __global__ void __launch_bounds__(512, OP == OL_OP_CUMULANT ? 2 : 1)
   // their loads are in flight while it is read
   const int64_t own0 = (L.block_offset + b) * BCELLS;
   if (L.prefetch_ahead > 0) prefetch_block_l2<ST>(L, b + L.prefetch_ahead, threadIdx.x);
+  pdl_wait();  // f_in, ghost rows: written by the launches before this one
   OwnRegs<ST> r;
   own_load(L.f_in, L.dstride, own0, threadIdx.x, r);
   const bool obs = L.obstacle[own0 + threadIdx.x] != 0;
@@ -106,7 +107,7 @@ static void launch_one(const LevelDev &L0, cudaStream_t s) {
   // level of fewer than four waves has little to hide and skips it
   LevelDev L = L0;
   L.prefetch_ahead = L.n_blocks >= 4 * resident ? resident * 3 / 4 : 0;
-  k_stream_collide<OP, ST, WALE><<<L.n_blocks, BCELLS, kStageBytes, s>>>(L);
+  launch_pdl(k_stream_collide<OP, ST, WALE>, L.n_blocks, BCELLS, kStageBytes, s, L);
 }
 
 template <int OP, bool WALE>
@@ -154,8 +155,8 @@ void launch_stream_collide(const LevelDev &L, bool f16, cudaStream_t s) {
   if (L.n_blocks <= 0) return;
   const int gn = L.gblocks ? L.n_gblocks : L.n_blocks;
   if (L.ghost && gn > 0) {
-    if (f16) k_ghost_fill<StoreF16S><<<gn, kGhostThreads, 0, s>>>(L);
-    else k_ghost_fill<StoreF32><<<gn, kGhostThreads, 0, s>>>(L);
+    if (f16) launch_pdl(k_ghost_fill<StoreF16S>, gn, kGhostThreads, 0, s, L);
+    else launch_pdl(k_ghost_fill<StoreF32>, gn, kGhostThreads, 0, s, L);
   }
   if (f16 || !use_pipeline()) {
     if (!f16) { launch_sc<StoreF32>(L, s); return; }

@@ -819,6 +819,7 @@ __device__ __forceinline__ void ghost_fill_block(const DEV &L, int b, float *G, 
 template <class ST>
 __global__ void __launch_bounds__(kGhostThreads, kGhostMinBlocks)
     k_ghost_fill(const __grid_constant__ LevelDev L) {
+  pdl_wait();  // the parent's new state and this level's f_in
   const int b = L.gblocks ? L.gblocks[blockIdx.x] : (int)blockIdx.x;
   ghost_fill_block<ST>(L, b, ghost_row_of(L, b), ghost_next_row_of(L, b));
 }
