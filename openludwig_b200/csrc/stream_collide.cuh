@@ -254,37 +254,38 @@ __device__ __noinline__ float pull_boundary(const LevelDev &L, int k, int b,
 // WALE eddy viscosity from vel_in central differences
 // (kernel_cumulant.jl:264-305, physics_utils.jl:85-123).
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ void vel_neighbor(const LevelDev &L, const int *nbbase,
-                                             int x, int y, int z, int dx,
-                                             int dy, int dz, float &ux, float &uy,
-                                             float &uz) {
-  int nx = x + dx, ny = y + dy, nz = z + dz;
-  const int ox = nx < 0 ? -1 : (nx > 7 ? 1 : 0);
-  const int oy = ny < 0 ? -1 : (ny > 7 ? 1 : 0);
-  const int oz = nz < 0 ? -1 : (nz > 7 ? 1 : 0);
-  const int nb = nbbase[(ox + 1) + 3 * (oy + 1) + 9 * (oz + 1)];
-  size_t ci;
-  if (nb >= 0) {
-    ci = (size_t)nb + (nx & 7) + BS * (ny & 7) + BS * BS * (nz & 7);
-  } else {
-    ci = (size_t)nbbase[13] + x + BS * y + BS * BS * z;
-  }
-  ux = __ldg(L.vel_in + ci);
-  uy = __ldg(L.vel_in + ci + L.dstride);
-  uz = __ldg(L.vel_in + ci + 2 * L.dstride);
+// Cell index of a face neighbour of the cell at local index `own` (element
+// offset, own block at nbbase[13]) one step along an axis: inside the block
+// `own + step`; across the face, the same cell of the face neighbour `dir`
+// (`own + wrap - nbbase[13] + nbbase[dir]`); with no neighbour there, the cell
+// itself (the zero-gradient fallback of physics_utils.jl:85-123).
+__device__ __forceinline__ int vel_neighbor(const int *nbbase, int own, bool inside, int step,
+                                            int dir, int wrap) {
+  if (inside) return own + step;
+  const int nb = nbbase[dir];
+  return nb >= 0 ? own - nbbase[13] + nb + wrap : own;
 }
 
 __device__ __forceinline__ float wale_nu(const LevelDev &L, const int *nbbase, int x, int y,
                                          int z) {
-  float exx, eyx, ezx, wxx, wyx, wzx;  // E (x+1), W (x-1)
-  float nxx, nyx, nzx, sxx, syx, szx;  // N (y+1), S (y-1)
-  float txx, tyx, tzx, bxx, byx, bzx;  // T (z+1), B (z-1)
-  vel_neighbor(L, nbbase, x, y, z, 1, 0, 0, exx, eyx, ezx);
-  vel_neighbor(L, nbbase, x, y, z, -1, 0, 0, wxx, wyx, wzx);
-  vel_neighbor(L, nbbase, x, y, z, 0, 1, 0, nxx, nyx, nzx);
-  vel_neighbor(L, nbbase, x, y, z, 0, -1, 0, sxx, syx, szx);
-  vel_neighbor(L, nbbase, x, y, z, 0, 0, 1, txx, tyx, tzx);
-  vel_neighbor(L, nbbase, x, y, z, 0, 0, -1, bxx, byx, bzx);
+  // the three velocity components are planes dstride apart
+  const float *__restrict__ v0 = L.vel_in;
+  const float *__restrict__ v1 = v0 + L.dstride;
+  const float *__restrict__ v2 = v1 + L.dstride;
+  const int own = nbbase[13] + x + BS * y + BS * BS * z;
+  // E (x+1), W (x-1), N (y+1), S (y-1), T (z+1), B (z-1)
+  const int ce = vel_neighbor(nbbase, own, x < BS - 1, 1, 14, -(BS - 1));
+  const int cw = vel_neighbor(nbbase, own, x > 0, -1, 12, BS - 1);
+  const int cn = vel_neighbor(nbbase, own, y < BS - 1, BS, 16, -BS * (BS - 1));
+  const int cs = vel_neighbor(nbbase, own, y > 0, -BS, 10, BS * (BS - 1));
+  const int ct = vel_neighbor(nbbase, own, z < BS - 1, BS * BS, 22, -BS * BS * (BS - 1));
+  const int cb = vel_neighbor(nbbase, own, z > 0, -BS * BS, 4, BS * BS * (BS - 1));
+  const float exx = __ldg(v0 + ce), eyx = __ldg(v1 + ce), ezx = __ldg(v2 + ce);
+  const float wxx = __ldg(v0 + cw), wyx = __ldg(v1 + cw), wzx = __ldg(v2 + cw);
+  const float nxx = __ldg(v0 + cn), nyx = __ldg(v1 + cn), nzx = __ldg(v2 + cn);
+  const float sxx = __ldg(v0 + cs), syx = __ldg(v1 + cs), szx = __ldg(v2 + cs);
+  const float txx = __ldg(v0 + ct), tyx = __ldg(v1 + ct), tzx = __ldg(v2 + ct);
+  const float bxx = __ldg(v0 + cb), byx = __ldg(v1 + cb), bzx = __ldg(v2 + cb);
   const float g11 = 0.5f * (exx - wxx), g12 = 0.5f * (nxx - sxx), g13 = 0.5f * (txx - bxx);
   const float g21 = 0.5f * (eyx - wyx), g22 = 0.5f * (nyx - syx), g23 = 0.5f * (tyx - byx);
   const float g31 = 0.5f * (ezx - wzx), g32 = 0.5f * (nzx - szx), g33 = 0.5f * (tzx - bzx);
