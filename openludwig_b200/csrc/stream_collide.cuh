@@ -886,15 +886,24 @@ __device__ __forceinline__ void own_load(const void *f_in_v, int64_t dstride, in
     if (k < 27) r.v[j] = __ldg((const uint4 *)(fin + (size_t)k * dstride + own + c0));
   }
 }
+// Odd lanes (x = 4..7 of a row) write their four cells rotated by one, so each
+// store instruction of a warp touches every bank at most twice (three times
+// in x order).
 __device__ __forceinline__ void own_store(const OwnRegs<StoreF32> &r, float, int t, float *E) {
   const int c0 = (t & 127) * 4;
   const int dst = e_index(c0 & 7, (c0 >> 3) & 7, c0 >> 6);
+  const bool odd = t & 1;
+  const int o0 = odd ? 1 : 0, o1 = odd ? 2 : 1, o2 = odd ? 3 : 2, o3 = odd ? 0 : 3;
 #pragma unroll
   for (int j = 0; j < 7; ++j) {
     const int k = (t >> 7) + 4 * j;
     if (k < 27) {
       float *e = E + k * EPL + dst;
-      e[0] = r.v[j].x; e[1] = r.v[j].y; e[2] = r.v[j].z; e[3] = r.v[j].w;
+      const float4 v = r.v[j];
+      e[o0] = odd ? v.y : v.x;
+      e[o1] = odd ? v.z : v.y;
+      e[o2] = odd ? v.w : v.z;
+      e[o3] = odd ? v.x : v.w;
     }
   }
 }
