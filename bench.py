@@ -35,6 +35,7 @@ import re
 import statistics
 import subprocess
 import sys
+import tempfile
 import time
 
 import numpy as np
@@ -60,21 +61,24 @@ class ClockSampler:
 
     NVML is polled from a thread every 10 ms (a read-only query), so that even
     a timed region of a few tens of milliseconds gets samples; `nvidia-smi
-    -lms 200` is the fallback when NVML cannot be opened.  Samples go to
-    gpurun_out/clocks_rank<i>.csv."""
+    -lms 200` is the fallback when NVML cannot be opened.  With `out_dir`
+    the samples are also written to <out_dir>/clocks_rank<i>.csv."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
     NAMES = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
 
-    def __init__(self, index: int, device=None):
+    def __init__(self, index: int, device=None, out_dir=None):
         self.index = index
+        self.out_dir = out_dir
         self.device = device
         self.proc = None
         self.thread = None
         self.samples = []          # (sm_mhz, max_mhz, reason names)
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{index}.csv")
+        self.path = os.path.join(out_dir or tempfile.gettempdir(),
+                                 f"clocks_rank{index}.csv" if out_dir else
+                                 f"ol_clocks_{os.getpid()}_rank{index}.csv")
 
     def _nvml_handle(self):
         import pynvml
@@ -124,10 +128,11 @@ class ClockSampler:
         if self.thread is not None:
             self.stop_flag.set()
             self.thread.join(timeout=5)
-            with open(self.path, "w") as fh:
-                fh.write("sm_mhz,max_sm_mhz,reasons\n")
-                for sm, mx, rs in self.samples:
-                    fh.write(f"{sm:.0f},{mx:.0f},{'|'.join(rs)}\n")
+            if self.out_dir:
+                with open(self.path, "w") as fh:
+                    fh.write("sm_mhz,max_sm_mhz,reasons\n")
+                    for sm, mx, rs in self.samples:
+                        fh.write(f"{sm:.0f},{mx:.0f},{'|'.join(rs)}\n")
             sm = [x[0] for x in self.samples]
             mx = [x[1] for x in self.samples]
             reasons = set(n for x in self.samples for n in x[2])
@@ -150,6 +155,8 @@ class ClockSampler:
                     if v.lower().startswith("active"):
                         reasons.add(nm)
             source = "nvidia-smi"
+            if not self.out_dir:
+                os.remove(self.path)
         else:
             sm, mx, reasons, source = [], [], set(), None
         if not sm:
@@ -225,6 +232,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="cube_3lvl")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--clocks-dir", default=None,
+                    help="also write the clock samples of the timed region to this directory")
     a = ap.parse_args()
     a.warmup = max(a.warmup, 3)
 
@@ -320,7 +329,7 @@ def main():
         graph.replay()
     torch.cuda.synchronize()
 
-    clk = ClockSampler(local, dev)
+    clk = ClockSampler(local, dev, a.clocks_dir)
     clk.start()
     if world > 1:
         dist.barrier()
