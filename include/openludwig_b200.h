@@ -142,6 +142,31 @@ typedef struct ol_step_params {
 OL_API int ol_stream_collide(const ol_level_view *lv, const ol_parent_view *pv,
                       const ol_step_params *sp, void *stream);
 
+/* Which kernel ol_stream_collide (and the block pool's stream-collide
+ * launches) run; no reference counterpart (the reference has one kernel
+ * launch shape).  OL_SC_KERNEL_BLOCK: one CTA per 8^3 block, synchronous
+ * staging.  OL_SC_KERNEL_WS: one persistent CTA per SM whose loader warps
+ * stage the next block while its consumer warps collide the current one
+ * (cumulant operator, levels whose absent-neighbour values are ghost rows or
+ * level-1 domain boundaries; other launches keep the per-block kernel).
+ * OL_SC_KERNEL_AUTO (default): OL_SC_KERNEL_WS for FP32 populations where
+ * it applies and the level has at least two blocks per SM.  Both kernels
+ * stage the same values and run the same cell-update code: rho and u agree
+ * bit for bit; a few post-collision populations may differ in the last bit
+ * (the compiler may fuse a multiply and an add differently in each).
+ * max_ctas > 0 caps the persistent grid (each CTA then walks more blocks;
+ * for tests of the stage hand-over), 0 = one CTA per SM.  Process-wide. */
+#define OL_SC_KERNEL_AUTO 0
+#define OL_SC_KERNEL_BLOCK 1
+#define OL_SC_KERNEL_WS 2
+OL_API int ol_set_stream_collide_kernel(int32_t choice, int32_t max_ctas);
+
+/* Reads and clears the fault bits of the current device's warp-specialised
+ * kernels: 1 = a consumer warp's wait for a staged block ran out, 2 = a
+ * loader warp's wait for a free stage ran out (each wait is bounded at 2 s;
+ * the kernel then ends early and its output is incomplete).  0 = none. */
+OL_API int ol_pipeline_fault(int32_t *flags);
+
 /* Bouzidi interpolated bounce-back (bouzidi_kernel.jl:13-122).  q_map holds
  * IEEE binary16 bit patterns [512*nB*27]; cell_* are the sparse boundary-cell
  * lists (block 1-based Int32, x/y/z 1-based Int8).  Reads f_post, writes f_out. */

@@ -94,5 +94,11 @@ struct WorkItem {
 // Per-device staging table of the 3176 out-of-block pull sources of a block
 // (built once on first use; see stage_block).
 const uint32_t *halo_table_device();
+// Per-device fault word of the warp-specialised kernels (null on failure).
+int *fault_word_device();
+// Current ol_set_stream_collide_kernel choice (OL_SC_KERNEL_*).
+int stream_collide_kernel_choice();
+// Grid of a warp-specialised launch over n_items work items.
+int ws_grid(int64_t n_items, int n_sm);
 
 }  // namespace ol

@@ -30,6 +30,7 @@
 
 #include "batched.cuh"
 #include "pipe.cuh"
+#include "ws.cuh"
 #include "common.cuh"
 #include "forces.cuh"
 
@@ -371,8 +372,10 @@ struct ol_ctx {
   cudaGraphExec_t exec = nullptr;
   bool dirty = true;
   // persistent grid = grid_mult * resident CTAs; 0 = one CTA per item;
-  // -1 = software-pipelined kernel (FP32 without DDF)
-  int grid_mult = 0;
+  // -1 = software-pipelined kernel (FP32 without DDF); -2 = warp-specialised
+  // persistent kernel (cumulant without DDF; the other variants then take
+  // one CTA per item)
+  int grid_mult = -2;
   int64_t launches = 0;
   double *d_out = nullptr;
   std::mutex mu;
@@ -512,9 +515,26 @@ static void free_plan(ol_ctx *c) {
 
 static int kernel_occupancy(int op) { return op == OL_OP_CUMULANT ? 2 : 1; }
 
+constexpr int kGridWs = -2;
+
 template <int OP, class ST, bool WALE, bool DDF>
 static void launch_variant(ol_ctx *c, const Launch &l) {
-  if (std::is_same<ST, StoreF32>::value && !DDF && c->grid_mult < 0) {
+  if constexpr (OP == OL_OP_CUMULANT && !DDF) {
+    // by default FP32 only: with FP16-shifted storage the warp-specialised
+    // kernel measured slower than one CTA per item (its consumers decode
+    // every landed value)
+    const int choice = stream_collide_kernel_choice();
+    const bool f32 = std::is_same<ST, StoreF32>::value;
+    if (choice == OL_SC_KERNEL_WS ||
+        (f32 && c->grid_mult == kGridWs && choice == OL_SC_KERNEL_AUTO)) {
+      const int grid = ws_grid(l.n, c->n_sm);
+      k_sc_ws<OP, ST, WALE, true><<<(unsigned)grid, kWsThreads, kWsBytes, c->stream>>>(
+          LevelDev{}, c->d_descs, c->d_items + l.off, (int)l.n, ws_table_device(),
+          fault_word_device());
+      return;
+    }
+  }
+  if (std::is_same<ST, StoreF32>::value && !DDF && c->grid_mult == -1) {
     // software-pipelined persistent kernel: all resident CTAs
     const int64_t grid = std::min<int64_t>(l.n, (int64_t)c->n_sm * kernel_occupancy(OP));
     k_sc_pipe<OP, WALE, true><<<(unsigned)grid, BCELLS, kPipeBytes, c->stream>>>(
@@ -522,7 +542,7 @@ static void launch_variant(ol_ctx *c, const Launch &l) {
     return;
   }
   const int64_t resident = (int64_t)c->n_sm * kernel_occupancy(OP);
-  int64_t grid = c->grid_mult == 0 ? l.n : std::min<int64_t>(l.n, resident * c->grid_mult);
+  int64_t grid = c->grid_mult <= 0 ? l.n : std::min<int64_t>(l.n, resident * c->grid_mult);
   if (grid < 1) grid = 1;
   k_sc_batched<OP, ST, WALE, DDF><<<(unsigned)grid, BCELLS, kStageBytes, c->stream>>>(
       c->d_descs, c->d_tdescs, c->d_items + l.off, (int)l.n);
@@ -808,6 +828,12 @@ static int prepare_attributes() {
   cudaFuncSetAttribute(k_sc_pipe<1, true, true>, (cudaFuncAttribute)a, kPipeBytes);
   prepare_attributes_st<StoreF32>();
   prepare_attributes_st<StoreF16S>();
+  cudaFuncSetAttribute(k_sc_ws<0, StoreF32, false, true>, (cudaFuncAttribute)a, kWsBytes);
+  cudaFuncSetAttribute(k_sc_ws<0, StoreF32, true, true>, (cudaFuncAttribute)a, kWsBytes);
+  cudaFuncSetAttribute(k_sc_ws<0, StoreF16S, false, true>, (cudaFuncAttribute)a, kWsBytes);
+  cudaFuncSetAttribute(k_sc_ws<0, StoreF16S, true, true>, (cudaFuncAttribute)a, kWsBytes);
+  if (!fault_word_device() || !ws_table_device())
+    return set_error(OL_ERR_CUDA, "warp-specialised kernel tables: allocation failed");
   const cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? OL_OK : cuda_status(e, "cudaFuncSetAttribute");
 }
@@ -1245,13 +1271,13 @@ extern "C" int ol_ctx_case_info(ol_ctx *c, int32_t id, int64_t *steps, int32_t *
 
 extern "C" int ol_ctx_autotune(ol_ctx *c, int32_t trials) {
   OL_CHECK_ARG(c && trials > 0, "ol_ctx_autotune: bad argument");
-  const int cands[4] = {0, 1, 2, -1};
+  const int cands[5] = {-2, 0, 1, 2, -1};
   float best_ms = 1e30f;
   int best = c->grid_mult;
   cudaEvent_t e0, e1;
   OL_CUDA(cudaEventCreate(&e0));
   OL_CUDA(cudaEventCreate(&e1));
-  for (int ci = 0; ci < 4; ++ci) {
+  for (int ci = 0; ci < 5; ++ci) {
     {
       std::lock_guard<std::mutex> lk(c->mu);
       c->grid_mult = cands[ci];

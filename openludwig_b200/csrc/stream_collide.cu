@@ -2,10 +2,12 @@
 // caller buffers in the reference layout (FP32 populations).
 #include <cstdlib>
 #include <mutex>
+#include <type_traits>
 #include <vector>
 
 #include "common.cuh"
 #include "pipe.cuh"
+#include "ws.cuh"
 
 namespace ol {
 
@@ -61,6 +63,90 @@ const uint32_t *halo_table_device() {
   return per_dev[dev];
 }
 
+// Loader table of the warp-specialised kernel (ws.cuh): the staging table's
+// out-of-block pulls in the same order, with the destination cell (the
+// pulling cell) in place of the 10^3 slot, then the face-halo velocity slots.
+static std::vector<uint32_t> build_ws_table() {
+  const std::vector<uint32_t> halo = build_halo_table();
+  std::vector<uint32_t> tab;
+  for (int i = 0; i < kHaloEntries; ++i) {
+    const uint32_t e = halo[i];
+    const int k = e & 31, slot = e >> 19;
+    const int dx = slot % 10 - 1 + cx_of(k), dy = (slot / 10) % 10 - 1 + cy_of(k),
+              dz = slot / 100 - 1 + cz_of(k);
+    const uint32_t d = (uint32_t)(dx + 8 * dy + 64 * dz);
+    tab.push_back((e & ((1u << 19) - 1)) | d << 19);
+  }
+  const int faces[6][3] = {{-1, 0, 0}, {1, 0, 0}, {0, -1, 0}, {0, 1, 0}, {0, 0, -1}, {0, 0, 1}};
+  for (const auto &f : faces) {
+    const uint32_t dir = (f[0] + 1) + 3 * (f[1] + 1) + 9 * (f[2] + 1);
+    for (int z = 0; z < 8; ++z)
+      for (int y = 0; y < 8; ++y)
+        for (int x = 0; x < 8; ++x) {
+          const bool on = (f[0] < 0 && x == 0) || (f[0] > 0 && x == 7) || (f[1] < 0 && y == 0) ||
+                          (f[1] > 0 && y == 7) || (f[2] < 0 && z == 0) || (f[2] > 0 && z == 7);
+          if (on) tab.push_back(dir | (uint32_t)(x + 8 * y + 64 * z) << 5);
+        }
+  }
+  return tab;
+}
+
+const uint32_t *ws_table_device() {
+  static std::mutex mu;
+  static uint32_t *per_dev[64] = {};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
+  std::lock_guard<std::mutex> lk(mu);
+  if (!per_dev[dev]) {
+    const std::vector<uint32_t> tab = build_ws_table();
+    if ((int)tab.size() != kWsTableSize) return nullptr;
+    uint32_t *d = nullptr;
+    if (cudaMalloc(&d, tab.size() * sizeof(uint32_t)) != cudaSuccess) return nullptr;
+    if (cudaMemcpy(d, tab.data(), tab.size() * sizeof(uint32_t), cudaMemcpyHostToDevice) !=
+        cudaSuccess) {
+      cudaFree(d);
+      return nullptr;
+    }
+    per_dev[dev] = d;
+  }
+  return per_dev[dev];
+}
+
+// Per-device fault word of the warp-specialised kernels (bits kWsFault*):
+// set when one of their bounded waits runs out; read and cleared by
+// ol_pipeline_fault.
+int *fault_word_device() {
+  static std::mutex mu;
+  static int *per_dev[64] = {};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
+  std::lock_guard<std::mutex> lk(mu);
+  if (!per_dev[dev]) {
+    int *d = nullptr;
+    if (cudaMalloc(&d, sizeof(int)) != cudaSuccess) return nullptr;
+    if (cudaMemset(d, 0, sizeof(int)) != cudaSuccess) {
+      cudaFree(d);
+      return nullptr;
+    }
+    per_dev[dev] = d;
+  }
+  return per_dev[dev];
+}
+
+// Stream-collide kernel selection (ol_set_stream_collide_kernel): 0 = by
+// level (warp-specialised persistent kernel where it applies and the level
+// spans at least two waves of it), 1 = one CTA per block, 2 = the
+// warp-specialised kernel wherever it applies.
+static int g_sc_kernel = OL_SC_KERNEL_AUTO;
+static int g_ws_max_ctas = 0;  // > 0: cap on the warp-specialised grid
+
+int stream_collide_kernel_choice() { return g_sc_kernel; }
+int ws_grid(int64_t n_items, int n_sm) {
+  int64_t g = n_items < n_sm ? n_items : n_sm;
+  if (g_ws_max_ctas > 0 && g > g_ws_max_ctas) g = g_ws_max_ctas;
+  return (int)(g < 1 ? 1 : g);
+}
+
 // One CTA per block: neighbour offsets, then the staged pull windows, then
 // the cell update.  Cumulant fits 64 registers (2 CTAs of 512 threads per
 // SM, 2 x 105 KB of staging); regularized BGK keeps 27 equilibria in flight
@@ -110,6 +196,49 @@ static void launch_one(const LevelDev &L0, cudaStream_t s) {
   launch_pdl(k_stream_collide<OP, ST, WALE>, L.n_blocks, BCELLS, kStageBytes, s, L);
 }
 
+// Warp-specialised persistent kernel over the level's blocks: one CTA per
+// SM (or per block when the level is smaller).
+template <int OP, class ST, bool WALE>
+static void launch_ws(const LevelDev &L, int n_sm, cudaStream_t s) {
+  static bool done = false;
+  if (!done) {
+    cudaFuncSetAttribute(k_sc_ws<OP, ST, WALE, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         kWsBytes);
+    done = true;
+  }
+  const int grid = ws_grid(L.n_blocks, n_sm);
+  launch_pdl(k_sc_ws<OP, ST, WALE, false>, grid, kWsThreads, kWsBytes, s, L,
+             (const LevelDev *)nullptr, (const WorkItem *)nullptr, 0, ws_table_device(),
+             fault_word_device());
+}
+
+static int device_sm_count() {
+  static int n_sm[64] = {};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 148;
+  if (!n_sm[dev]) {
+    int v = 0;
+    if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || v <= 0)
+      v = 148;
+    n_sm[dev] = v;
+  }
+  return n_sm[dev];
+}
+
+// Whether the warp-specialised kernel serves this level: cumulant operator;
+// every absent-neighbour value either precomputed in ghost rows or a
+// level-1 domain-boundary value its loader evaluates; the arrays it moves
+// with bulk copies 16-byte aligned.
+static bool ws_applies(const LevelDev &L) {
+  auto a16 = [](const void *p) { return ((uintptr_t)p & 15) == 0; };
+  if (L.sp.op != OL_OP_CUMULANT) return false;
+  if (!L.sp.is_level_1 && !L.ghost) return false;
+  if (!a16(L.f_in) || !a16(L.obstacle) || !a16(L.sponge)) return false;
+  if (L.sp.c_wale != 0.0f && !a16(L.vel_in)) return false;
+  if (L.sp.wall_model_active == 1 && L.wall_dist && !a16(L.wall_dist)) return false;
+  return fault_word_device() != nullptr && ws_table_device() != nullptr;
+}
+
 template <int OP, bool WALE>
 static void launch_pipe(const LevelDev &L, cudaStream_t s) {
   static bool done = false;
@@ -130,6 +259,15 @@ static void launch_pipe(const LevelDev &L, cudaStream_t s) {
 template <class ST>
 static void launch_sc(const LevelDev &L, cudaStream_t s) {
   const bool wale = L.sp.c_wale != 0.0f;
+  const int n_sm = device_sm_count();
+  const bool ws = g_sc_kernel == OL_SC_KERNEL_WS ||
+                  (g_sc_kernel == OL_SC_KERNEL_AUTO && L.n_blocks >= 2 * n_sm &&
+                   std::is_same<ST, StoreF32>::value);
+  if (ws && ws_applies(L)) {
+    if (wale) launch_ws<OL_OP_CUMULANT, ST, true>(L, n_sm, s);
+    else launch_ws<OL_OP_CUMULANT, ST, false>(L, n_sm, s);
+    return;
+  }
   if (L.sp.op == OL_OP_CUMULANT) {
     if (wale) launch_one<OL_OP_CUMULANT, ST, true>(L, s);
     else launch_one<OL_OP_CUMULANT, ST, false>(L, s);
@@ -261,6 +399,27 @@ extern "C" int ol_stream_collide(const ol_level_view *lv, const ol_parent_view *
   }
   launch_stream_collide(L, false, (cudaStream_t)stream);
   OL_LAUNCHED("ol_stream_collide");
+  return OL_OK;
+}
+
+extern "C" int ol_set_stream_collide_kernel(int32_t choice, int32_t max_ctas) {
+  OL_CHECK_ARG(choice == OL_SC_KERNEL_AUTO || choice == OL_SC_KERNEL_BLOCK ||
+                   choice == OL_SC_KERNEL_WS,
+               "ol_set_stream_collide_kernel: unknown choice %d", choice);
+  OL_CHECK_ARG(max_ctas >= 0, "ol_set_stream_collide_kernel: max_ctas < 0");
+  g_sc_kernel = choice;
+  g_ws_max_ctas = max_ctas;
+  return OL_OK;
+}
+
+extern "C" int ol_pipeline_fault(int32_t *flags) {
+  OL_CHECK_ARG(flags, "ol_pipeline_fault: null output");
+  int *d = fault_word_device();
+  if (!d) return set_error(OL_ERR_CUDA, "ol_pipeline_fault: fault word allocation failed");
+  int v = 0;
+  OL_CUDA(cudaMemcpy(&v, d, sizeof(int), cudaMemcpyDeviceToHost));
+  OL_CUDA(cudaMemset(d, 0, sizeof(int)));
+  *flags = v;
   return OL_OK;
 }
 

@@ -266,8 +266,14 @@ __device__ __forceinline__ int vel_neighbor(const int *nbbase, int own, bool ins
   return nb >= 0 ? own - nbbase[13] + nb + wrap : own;
 }
 
-__device__ __forceinline__ float wale_nu(const LevelDev &L, const int *nbbase, int x, int y,
-                                         int z) {
+// The 18 neighbour velocities the WALE gradients need (E, W, N, S, T, B
+// neighbour, x/y/z component each), read from vel_in.
+struct WaleVel {
+  float e[3], w[3], n[3], s[3], t[3], b[3];
+};
+
+__device__ __forceinline__ void wale_load(const LevelDev &L, const int *nbbase, int x, int y, int z,
+                                          WaleVel &V) {
   // the three velocity components are planes dstride apart
   const float *__restrict__ v0 = L.vel_in;
   const float *__restrict__ v1 = v0 + L.dstride;
@@ -280,12 +286,21 @@ __device__ __forceinline__ float wale_nu(const LevelDev &L, const int *nbbase, i
   const int cs = vel_neighbor(nbbase, own, y > 0, -BS, 10, BS * (BS - 1));
   const int ct = vel_neighbor(nbbase, own, z < BS - 1, BS * BS, 22, -BS * BS * (BS - 1));
   const int cb = vel_neighbor(nbbase, own, z > 0, -BS * BS, 4, BS * BS * (BS - 1));
-  const float exx = __ldg(v0 + ce), eyx = __ldg(v1 + ce), ezx = __ldg(v2 + ce);
-  const float wxx = __ldg(v0 + cw), wyx = __ldg(v1 + cw), wzx = __ldg(v2 + cw);
-  const float nxx = __ldg(v0 + cn), nyx = __ldg(v1 + cn), nzx = __ldg(v2 + cn);
-  const float sxx = __ldg(v0 + cs), syx = __ldg(v1 + cs), szx = __ldg(v2 + cs);
-  const float txx = __ldg(v0 + ct), tyx = __ldg(v1 + ct), tzx = __ldg(v2 + ct);
-  const float bxx = __ldg(v0 + cb), byx = __ldg(v1 + cb), bzx = __ldg(v2 + cb);
+  V.e[0] = __ldg(v0 + ce); V.e[1] = __ldg(v1 + ce); V.e[2] = __ldg(v2 + ce);
+  V.w[0] = __ldg(v0 + cw); V.w[1] = __ldg(v1 + cw); V.w[2] = __ldg(v2 + cw);
+  V.n[0] = __ldg(v0 + cn); V.n[1] = __ldg(v1 + cn); V.n[2] = __ldg(v2 + cn);
+  V.s[0] = __ldg(v0 + cs); V.s[1] = __ldg(v1 + cs); V.s[2] = __ldg(v2 + cs);
+  V.t[0] = __ldg(v0 + ct); V.t[1] = __ldg(v1 + ct); V.t[2] = __ldg(v2 + ct);
+  V.b[0] = __ldg(v0 + cb); V.b[1] = __ldg(v1 + cb); V.b[2] = __ldg(v2 + cb);
+}
+
+__device__ __forceinline__ float wale_from(const WaleVel &V, float c_wale) {
+  const float exx = V.e[0], eyx = V.e[1], ezx = V.e[2];
+  const float wxx = V.w[0], wyx = V.w[1], wzx = V.w[2];
+  const float nxx = V.n[0], nyx = V.n[1], nzx = V.n[2];
+  const float sxx = V.s[0], syx = V.s[1], szx = V.s[2];
+  const float txx = V.t[0], tyx = V.t[1], tzx = V.t[2];
+  const float bxx = V.b[0], byx = V.b[1], bzx = V.b[2];
   const float g11 = 0.5f * (exx - wxx), g12 = 0.5f * (nxx - sxx), g13 = 0.5f * (txx - bxx);
   const float g21 = 0.5f * (eyx - wyx), g22 = 0.5f * (nyx - syx), g23 = 0.5f * (tyx - byx);
   const float g31 = 0.5f * (ezx - wzx), g32 = 0.5f * (nzx - szx), g33 = 0.5f * (tzx - bzx);
@@ -313,9 +328,16 @@ __device__ __forceinline__ float wale_nu(const LevelDev &L, const int *nbbase, i
     const float op1_32 = OP1 * sqrtf(OP1);
     const float op2_52 = OP2 * OP2 * sqrtf(fmaxf(OP2, 1e-12f));
     const float den = op2_52 + OP1 * sqrtf(sqrtf(fmaxf(OP1, 1e-12f)));
-    if (den > 1e-12f) nu = (L.sp.c_wale * L.sp.c_wale) * op1_32 / den;
+    if (den > 1e-12f) nu = (c_wale * c_wale) * op1_32 / den;
   }
   return nu;
+}
+
+__device__ __forceinline__ float wale_nu(const LevelDev &L, const int *nbbase, int x, int y,
+                                         int z) {
+  WaleVel V;
+  wale_load(L, nbbase, x, y, z, V);
+  return wale_from(V, L.sp.c_wale);
 }
 
 // ---------------------------------------------------------------------------
@@ -1023,9 +1045,18 @@ __device__ __forceinline__ void load_pulls(const float *E, int t, float (&A)[27]
     A[k] = E[k * EPL + eb - (cx_of(k) + 10 * cy_of(k) + 100 * cz_of(k))];
 }
 
+// Per-cell inputs a caller may have read ahead of the collision (the
+// warp-specialised kernel issues them before its shared-memory pulls):
+// the wall distance and the WALE neighbour velocities.
+struct CellAux {
+  float wall_dist;
+  WaleVel wale;
+};
+
 template <int OP, class ST, bool WALE>
 __device__ __forceinline__ void collide_cell(const LevelDev &L, const int *nbbase, float (&A)[27],
-                                             int b, int t, bool obs, float spg);
+                                             int b, int t, bool obs, float spg,
+                                             const CellAux *aux = nullptr);
 
 template <int OP, class ST, bool WALE>
 __device__ __forceinline__ void stream_collide_cell(const LevelDev &L, const int *nbbase,
@@ -1040,7 +1071,8 @@ __device__ __forceinline__ void stream_collide_cell(const LevelDev &L, const int
 // WALE, collision, forcing and the stores of cell t of block b.
 template <int OP, class ST, bool WALE>
 __device__ __forceinline__ void collide_cell(const LevelDev &L, const int *nbbase, float (&A)[27],
-                                             int b, int t, bool obs, float spg) {
+                                             int b, int t, bool obs, float spg,
+                                             const CellAux *aux) {
   using T = typename ST::T;
   const int x = t & 7, y = (t >> 3) & 7, z = t >> 6;
   const ol_step_params &sp = L.sp;
@@ -1093,7 +1125,8 @@ __device__ __forceinline__ void collide_cell(const LevelDev &L, const int *nbbas
   }
   float Fx = 0.0f, Fy = 0.0f, Fz = 0.0f;
   if (sp.wall_model_active == 1 && L.wall_dist)
-    wall_force(L.wall_dist[own], rho, ux, uy, uz, sp.tau_molecular, Fx, Fy, Fz);
+    wall_force(aux ? aux->wall_dist : L.wall_dist[own], rho, ux, uy, uz, sp.tau_molecular, Fx,
+               Fy, Fz);
   const bool forced = (Fx != 0.0f) | (Fy != 0.0f) | (Fz != 0.0f);
   const float uxe = ux + 0.5f * Fx * inv_rho;
   const float uye = uy + 0.5f * Fy * inv_rho;
@@ -1105,7 +1138,7 @@ __device__ __forceinline__ void collide_cell(const LevelDev &L, const int *nbbas
   L.rho_out[own] = rho;
 
   float nu_eddy = 0.0f;
-  if (WALE) nu_eddy = wale_nu(L, nbbase, x, y, z);
+  if (WALE) nu_eddy = aux ? wale_from(aux->wale, sp.c_wale) : wale_nu(L, nbbase, x, y, z);
   nu_eddy = fmaxf(nu_eddy, sp.nu_sgs_background);
 
   float omega;  // omega_1 (cumulant) or omega (BGK)
