@@ -225,10 +225,11 @@ OL_API int ol_bouzidi_apply_links(float *f_out, const ol_bouzidi_link *links, in
  * OL_BOUZIDI_NOALLOC_MAX_CELLS boundary cells (27 floats each, 7 MB, held by
  * every device that loads the library until exit); larger n_boundary is
  * rejected with OL_ERR_ARG.  The call allocates nothing.  Its first call on
- * a device looks up the array's device address (once per device, that
- * device current); make that first call before any stream capture.  All
- * calls share the one array: calls that overlap on the GPU (other streams,
- * other host threads) race on it. */
+ * a device looks up the array's device address (once per device and CUDA
+ * context, that device current; after a device reset or under another
+ * context the next call looks it up again); make that first call before any
+ * stream capture.  All calls share the one array: calls that overlap on the
+ * GPU (other streams, other host threads) race on it. */
 #define OL_BOUZIDI_NOALLOC_MAX_CELLS 65536
 OL_API int ol_bouzidi_sparse_noalloc(float *f_out, const uint16_t *q_map,
                       const int32_t *cell_block, const int8_t *cell_x,
@@ -458,8 +459,24 @@ OL_API int ol_ctx_case_download_thermal(ol_ctx *ctx, int32_t case_id, int32_t le
 /* Coarse steps a case has done, and its device watchdog status. */
 OL_API int ol_ctx_case_info(ol_ctx *ctx, int32_t case_id, int64_t *coarse_steps,
                      int32_t *status);
-/* Launch-shape autotuning over persistent grid sizes; result is kept.
- * Timing replays advance every resident case by 4 * (trials + 1) steps. */
+/* Launch shape of the context's stream-collide launches (no reference
+ * counterpart):
+ *   OL_LAUNCH_WS         warp-specialised persistent kernel, one CTA per SM
+ *                        (FP32 cumulant launches without DDF; the other
+ *                        variants take one CTA per work item) -- default;
+ *   OL_LAUNCH_PIPELINED  software-pipelined persistent kernel (FP32 without
+ *                        DDF), two CTAs per SM;
+ *   OL_LAUNCH_PER_ITEM   one CTA per (case, level, block) work item;
+ *   1, 2                 persistent grid of 1x / 2x the resident CTAs.
+ * Every shape runs the same cell update on the same staged values. */
+#define OL_LAUNCH_WS (-2)
+#define OL_LAUNCH_PIPELINED (-1)
+#define OL_LAUNCH_PER_ITEM 0
+OL_API int ol_ctx_set_launch(ol_ctx *ctx, int32_t shape);
+OL_API int ol_ctx_get_launch(ol_ctx *ctx, int32_t *shape);
+/* Times one coarse step of the resident mix (CUDA events) under each launch
+ * shape above and keeps the fastest.  The timing replays advance every
+ * resident case by 5 * (trials + 1) coarse steps. */
 OL_API int ol_ctx_autotune(ol_ctx *ctx, int32_t trials);
 /* Bytes in use / budget / number of resident cases / kernel launches issued. */
 OL_API int ol_ctx_stats(ol_ctx *ctx, size_t *used, size_t *budget, int32_t *n_cases,

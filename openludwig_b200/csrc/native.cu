@@ -1269,9 +1269,24 @@ extern "C" int ol_ctx_case_info(ol_ctx *c, int32_t id, int64_t *steps, int32_t *
   return OL_OK;
 }
 
+extern "C" int ol_ctx_set_launch(ol_ctx *c, int32_t shape) {
+  OL_CHECK_ARG(c, "ol_ctx_set_launch: null context");
+  OL_CHECK_ARG(shape >= OL_LAUNCH_WS && shape <= 2, "ol_ctx_set_launch: unknown shape %d", shape);
+  std::lock_guard<std::mutex> lk(c->mu);
+  c->grid_mult = shape;
+  c->dirty = true;
+  return OL_OK;
+}
+
+extern "C" int ol_ctx_get_launch(ol_ctx *c, int32_t *shape) {
+  OL_CHECK_ARG(c && shape, "ol_ctx_get_launch: null argument");
+  *shape = c->grid_mult;
+  return OL_OK;
+}
+
 extern "C" int ol_ctx_autotune(ol_ctx *c, int32_t trials) {
   OL_CHECK_ARG(c && trials > 0, "ol_ctx_autotune: bad argument");
-  const int cands[5] = {-2, 0, 1, 2, -1};
+  const int cands[5] = {OL_LAUNCH_WS, OL_LAUNCH_PER_ITEM, 1, 2, OL_LAUNCH_PIPELINED};
   float best_ms = 1e30f;
   int best = c->grid_mult;
   cudaEvent_t e0, e1;

@@ -8,6 +8,8 @@
 // cudaMalloc can fail even though the pool has room, or they run a loop that
 // must not allocate at all.  This variant keeps the scratch in a file-scope
 // device array of fixed size instead, so a call allocates nothing.
+#include <cuda.h>  // driver types only; the entry points are fetched at run time
+
 #include <mutex>
 
 #include "bouzidi.cuh"
@@ -18,20 +20,61 @@ namespace ol {
 // Resident on every device that loads the library, until process exit.
 static __device__ __align__(256) float g_bouzidi_scratch[(size_t)OL_BOUZIDI_NOALLOC_MAX_CELLS * 27];
 
+// Unique id of the calling thread's current CUDA context (0 when none is
+// current yet), through the driver's cuCtxGetCurrent / cuCtxGetId, fetched
+// from the runtime once (the library links only the static runtime).
+static int current_context_id(unsigned long long *id) {
+  using GetCurrent = CUresult (*)(CUcontext *);
+  using GetId = CUresult (*)(CUcontext, unsigned long long *);
+  static GetCurrent get_current = nullptr;
+  static GetId get_id = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    cudaDriverEntryPointQueryResult q{};
+    void *p = nullptr;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_current = (GetCurrent)p;
+    p = nullptr;
+    if (cudaGetDriverEntryPoint("cuCtxGetId", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_id = (GetId)p;
+  });
+  if (!get_current || !get_id)
+    return set_error(OL_ERR_CUDA, "ol_bouzidi_sparse_noalloc: driver context queries unavailable");
+  CUcontext ctx = nullptr;
+  if (get_current(&ctx) != CUDA_SUCCESS)
+    return set_error(OL_ERR_CUDA, "ol_bouzidi_sparse_noalloc: cuCtxGetCurrent failed");
+  *id = 0;
+  if (ctx && get_id(ctx, id) != CUDA_SUCCESS)
+    return set_error(OL_ERR_CUDA, "ol_bouzidi_sparse_noalloc: cuCtxGetId failed");
+  return OL_OK;
+}
+
 // The array's name is only a host-side stand-in in host code; the kernels
-// need its device address, looked up once per device with that device current.
+// need its device address, looked up with the device current.  The address
+// is kept per device together with the id of the context it belongs to and
+// looked up again when the current context is another one (after a device
+// reset, or a context the caller created itself).
 static int noalloc_scratch(float **out) {
   static std::mutex mu;
   static float *per_dev[64] = {};
+  static unsigned long long ctx_of[64] = {};
   int dev = 0;
   OL_CUDA(cudaGetDevice(&dev));
   OL_CHECK_ARG(dev >= 0 && dev < 64, "ol_bouzidi_sparse_noalloc: device id %d out of range", dev);
+  unsigned long long id = 0;
+  int rc = current_context_id(&id);
+  if (rc) return rc;
   std::lock_guard<std::mutex> lk(mu);
-  if (!per_dev[dev]) {
+  if (!per_dev[dev] || id == 0 || ctx_of[dev] != id) {
     void *p = nullptr;
     const cudaError_t e = cudaGetSymbolAddress(&p, g_bouzidi_scratch);
     if (e != cudaSuccess) return cuda_status(e, "cudaGetSymbolAddress(g_bouzidi_scratch)");
+    // the lookup makes the device's primary context current if none was
+    if (id == 0 && (rc = current_context_id(&id))) return rc;
     per_dev[dev] = (float *)p;
+    ctx_of[dev] = id;
   }
   *out = per_dev[dev];
   return OL_OK;

@@ -281,6 +281,15 @@ class Context:
     def autotune(self, trials: int = 3) -> None:
         N.call("ol_ctx_autotune", self._h, trials)
 
+    def set_launch(self, shape: int) -> None:
+        """Launch shape of the stream-collide launches (OL_LAUNCH_*, 1, 2)."""
+        N.call("ol_ctx_set_launch", self._h, shape)
+
+    def launch(self) -> int:
+        out = C.c_int32()
+        N.call("ol_ctx_get_launch", self._h, C.byref(out))
+        return int(out.value)
+
     def stats(self) -> dict:
         used, budget = C.c_size_t(), C.c_size_t()
         n, launches = C.c_int32(), C.c_int64()

@@ -8,11 +8,13 @@ from them: the configuration values config_loader.jl:133-281 would set (the
 expected values below were read off the YAML text and the defaults in
 config_loader.jl:5-119), the facet count and bounds of the parsed STL
 (geometry.jl:385-429) and the triangle count after longest-edge subdivision
-(geometry.jl:174-258).  Run it from the repository root:
+(geometry.jl:174-258).  Run it from the repository root, naming the
+reference checkout as the argument or in OL_REFERENCE_ROOT:
 
     python tests/golden/make_golden.py /path/to/reference
 """
 import json
+import os
 import sys
 from pathlib import Path
 
@@ -50,4 +52,7 @@ def main(ref: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("OL_REFERENCE_ROOT")
+    if not ref:
+        sys.exit("usage: make_golden.py REFERENCE_ROOT (or set OL_REFERENCE_ROOT)")
+    main(ref)

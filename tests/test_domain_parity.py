@@ -71,6 +71,26 @@ def test_rotated_cube_three_levels_matches_oracle():
         assert all(((x + 1) // 2, (y + 1) // 2, (z + 1) // 2) in par for x, y, z in b.coords.tolist())
 
 
+def test_cube_3lvl_full_size_matches_oracle():
+    """The benchmark workload's own domain (cube side 64 finest cells, three
+    levels of 2000 / 1728 / 4608 blocks): every level's block set and order,
+    neighbour table, voxels, flood fill, sponge, wall distance and the finest
+    level's Bouzidi q-map, triangle ids and boundary cells, bit for bit."""
+    c, mesh = workloads.cube_3lvl()
+    p = scaling.compute_domain_from_mesh(c, mesh.min_bounds, mesh.max_bounds)
+    hosts = domain.setup_multilevel_domain(c, mesh, p)
+    assert [h.n_blocks for h in hosts] == [2000, 1728, 4608]
+    assert (p.nx_coarse, p.ny_coarse, p.nz_coarse) == (160, 80, 80)
+    prev = None
+    for i, h in enumerate(hosts):
+        scale = 2 ** i
+        dims = (p.bx_max * scale, p.by_max * scale, p.bz_max * scale)
+        prev_bs = 8 * (p.dx_coarse / 2 ** (i - 1)) if i > 0 else 0.0
+        prev = _compare_level(h, mesh.triangles, p.dx_coarse / scale, p.mesh_offset, dims, prev,
+                              prev_bs, sponge_args=(p.domain_size, c.sponge_thickness, False))
+    assert hosts[-1].bouzidi and hosts[-1].n_boundary > 0
+
+
 def test_wing_voxelization_and_qmap_match_oracle():
     """Thin closed NACA0012 wing (coarse panels) on one level."""
     mesh = geo.rotate_mesh(geo.naca0012_wing(1.0, 1.0, n_chord=24, n_span=4), 6.0, -3.0)
