@@ -18,10 +18,11 @@
  * convention (block ids 1..nB, 0 = missing; Bouzidi cell x/y/z in 1..8).
  * The block edge is fixed at 8 cells (blocks.jl BLOCK_SIZE).
  *
- * Native layer (ol_ctx_*, ol_batch_*): the library owns a device block pool
- * with FP32 or FP16-shifted population storage, advances many cases of uneven
- * size together with persistent kernels replayed from a CUDA graph, and is
- * driven by the Python request loop in openludwig_b200.serving.
+ * Native layer (ol_ctx_*): the library owns a device block pool with FP32 or
+ * FP16-shifted population storage and advances many cases of uneven size
+ * together with persistent kernels replayed from a CUDA graph; ol_server_* /
+ * ol_serve_* run the continuous-batching request loop over it (driven from
+ * Python by openludwig_b200.serving, or from any caller of the C ABI).
  */
 #ifndef OPENLUDWIG_B200_H
 #define OPENLUDWIG_B200_H
@@ -448,6 +449,31 @@ OL_API int ol_ctx_sync(ol_ctx *ctx);
 OL_API int ol_ctx_step_timed(ol_ctx *ctx, int32_t n_coarse, float *ms);
 /* Surface forces of one case on its finest level: out[9] as ol_surface_forces. */
 OL_API int ol_ctx_case_forces(ol_ctx *ctx, int32_t case_id, double out[9]);
+
+/* Reference values of the force coefficients (surface.jl:873-910): free-
+ * stream density and speed, reference area and chord (physical units, as
+ * the force sums), and whether the case is a half model (symmetric). */
+typedef struct ol_coeff_ref {
+  double rho_ref, u_ref, area_ref, chord_ref;
+  int32_t symmetric;
+} ol_coeff_ref;
+
+/* The coefficient record of one case (compute_aerodynamics!, surface.jl:
+ * 913-920, with the finishing of integrate_surface_forces!, :873-910):
+ * out[12] = {Cd, Cl, Cs, Cmx, Cmy, Cmz, Fx, Fy, Fz, Mx, My, Mz} -- Cd along
+ * x, Cl along z, Cs along y; forces are pressure + viscous, moments about
+ * the moment centre, after symmetry doubling of a half model. */
+OL_API int ol_ctx_case_coefficients(ol_ctx *ctx, int32_t case_id, const ol_coeff_ref *ref,
+                                    double out[12]);
+
+/* Advance ONE resident case by n_coarse coarse steps (the per-case
+ * counterpart of ol_ctx_step; the reference steps its single case with
+ * execute_timestep_batch!, solver_control.jl:199-218).  u_in >= 0 fixes
+ * the case's inlet speed (lattice units) from now on, replacing its ramp;
+ * u_in < 0 keeps the case's target and ramp.  The other resident cases do
+ * not move.  It replays a graph of this case alone, so the next ol_ctx_step
+ * rebuilds the graph of all cases. */
+OL_API int ol_ctx_case_step(ol_ctx *ctx, int32_t case_id, int32_t n_coarse, float u_in);
 /* Download a level's macroscopic fields (host buffers of 512*nB / 512*nB*3),
  * populations (host [512*nB*27] FP32, decoded), or NULL to skip. */
 OL_API int ol_ctx_case_download(ol_ctx *ctx, int32_t case_id, int32_t level,
@@ -478,6 +504,54 @@ OL_API int ol_ctx_get_launch(ol_ctx *ctx, int32_t *shape);
  * shape above and keeps the fastest.  The timing replays advance every
  * resident case by 5 * (trials + 1) coarse steps. */
 OL_API int ol_ctx_autotune(ol_ctx *ctx, int32_t trials);
+/* ------------------------------------------------------------------ */
+/* Serving: continuous batching of solve requests over one context      */
+/* ------------------------------------------------------------------ */
+/* No reference counterpart beyond its sequential multi-case loop
+ * (run_all_cases, main.jl:413-466).  Requests are admitted in arrival order
+ * as soon as their footprint fits the context's budget; all resident cases
+ * step together, check_every coarse steps per ol_serve_advance; a case
+ * retires when |Cd(t) - Cd(t - window)| < tol after at least min_steps, on
+ * its watchdog's non-finite flag, at max_steps, or when Cd is not finite. */
+typedef struct ol_serve_rule {
+  int32_t check_every;   /* coarse steps between Cd checks                */
+  int32_t window;        /* convergence window, a multiple of check_every */
+  double tol;            /* |Cd(t) - Cd(t - window)| bound                */
+  int32_t max_steps;     /* retire anyway after this many coarse steps    */
+  int32_t min_steps;     /* no convergence retirement before this         */
+} ol_serve_rule;
+
+/* One retired request.  Times on the server clock (seconds). */
+typedef struct ol_serve_result {
+  int32_t rid;
+  int32_t steps;         /* coarse steps done                              */
+  int32_t status;        /* device watchdog bits                           */
+  int32_t converged;     /* 1 if retired by the convergence rule           */
+  double arrival_s, admit_s, finish_s;
+  double coeff[12];      /* last check's record, as ol_ctx_case_coefficients */
+} ol_serve_result;
+
+typedef struct ol_server ol_server;
+OL_API int ol_server_create(ol_server **out, ol_ctx *ctx, const ol_serve_rule *rule);
+/* Removes the cases still resident; the context stays. */
+OL_API int ol_server_destroy(ol_server *srv);
+/* Seconds since the server was created (steady clock). */
+OL_API int ol_server_clock(ol_server *srv, double *now_s);
+/* Queues a request arriving at arrival_s (server clock).  The descriptor and
+ * the host arrays it points to must stay valid until the request's result
+ * has been polled.  Fails with OL_ERR_NOMEM if the case can never fit. */
+OL_API int ol_serve_submit(ol_server *srv, const ol_case_desc *cd, const ol_coeff_ref *ref,
+                           double arrival_s, int32_t *rid);
+/* One round: admit what has arrived and fits, then (if any case is
+ * resident) step check_every coarse steps, check Cd, retire.  Synchronous.
+ * Reports how many requests are resident and queued afterwards. */
+OL_API int ol_serve_advance(ol_server *srv, int32_t *n_resident, int32_t *n_queued);
+/* Up to `max` retired requests not yet polled, oldest first. */
+OL_API int ol_serve_poll(ol_server *srv, ol_serve_result *out, int32_t max, int32_t *n);
+/* The Cd check history of a retired request (*n = its length; up to `max`
+ * values copied). */
+OL_API int ol_serve_history(ol_server *srv, int32_t rid, double *cd, int32_t max, int32_t *n);
+
 /* Bytes in use / budget / number of resident cases / kernel launches issued. */
 OL_API int ol_ctx_stats(ol_ctx *ctx, size_t *used, size_t *budget, int32_t *n_cases,
                  int64_t *launches);

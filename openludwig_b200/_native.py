@@ -133,6 +133,26 @@ class CaseDesc(C.Structure):
                 ("async_depth", i32), ("q_min_threshold", f32), ("T_initial", f32)]
 
 
+class CoeffRef(C.Structure):
+    _fields_ = [("rho_ref", C.c_double), ("u_ref", C.c_double), ("area_ref", C.c_double),
+                ("chord_ref", C.c_double), ("symmetric", i32)]
+
+
+class ServeRule(C.Structure):
+    _fields_ = [("check_every", i32), ("window", i32), ("tol", C.c_double),
+                ("max_steps", i32), ("min_steps", i32)]
+
+
+class ServeResult(C.Structure):
+    _fields_ = [("rid", i32), ("steps", i32), ("status", i32), ("converged", i32),
+                ("arrival_s", C.c_double), ("admit_s", C.c_double), ("finish_s", C.c_double),
+                ("coeff", C.c_double * 12)]
+
+
+OL_SC_KERNEL_AUTO, OL_SC_KERNEL_BLOCK, OL_SC_KERNEL_WS = 0, 1, 2
+OL_LAUNCH_WS, OL_LAUNCH_PIPELINED, OL_LAUNCH_PER_ITEM = -2, -1, 0
+
+
 class OLError(RuntimeError):
     """A C-ABI call returned a non-zero status."""
 
@@ -184,6 +204,20 @@ _SIGS = {
     "ol_ctx_case_download_thermal": (C.c_int, [vp, i32, i32, vp, vp]),
     "ol_ctx_case_info": (C.c_int, [vp, i32, C.POINTER(C.c_int64), C.POINTER(i32)]),
     "ol_ctx_autotune": (C.c_int, [vp, i32]),
+    "ol_ctx_set_launch": (C.c_int, [vp, i32]),
+    "ol_ctx_get_launch": (C.c_int, [vp, C.POINTER(i32)]),
+    "ol_ctx_case_step": (C.c_int, [vp, i32, i32, f32]),
+    "ol_ctx_case_coefficients": (C.c_int, [vp, i32, C.POINTER(CoeffRef), C.POINTER(C.c_double)]),
+    "ol_set_stream_collide_kernel": (C.c_int, [i32, i32]),
+    "ol_pipeline_fault": (C.c_int, [C.POINTER(i32)]),
+    "ol_server_create": (C.c_int, [C.POINTER(vp), vp, C.POINTER(ServeRule)]),
+    "ol_server_destroy": (C.c_int, [vp]),
+    "ol_server_clock": (C.c_int, [vp, C.POINTER(C.c_double)]),
+    "ol_serve_submit": (C.c_int, [vp, C.POINTER(CaseDesc), C.POINTER(CoeffRef), C.c_double,
+                                  C.POINTER(i32)]),
+    "ol_serve_advance": (C.c_int, [vp, C.POINTER(i32), C.POINTER(i32)]),
+    "ol_serve_poll": (C.c_int, [vp, C.POINTER(ServeResult), i32, C.POINTER(i32)]),
+    "ol_serve_history": (C.c_int, [vp, i32, C.POINTER(C.c_double), i32, C.POINTER(i32)]),
     "ol_ctx_stats": (C.c_int, [vp, C.POINTER(C.c_size_t), C.POINTER(C.c_size_t),
                                C.POINTER(i32), C.POINTER(C.c_int64)]),
     "ol_last_error": (C.c_char_p, []),

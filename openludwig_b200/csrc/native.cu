@@ -29,6 +29,7 @@
 #include <vector>
 
 #include "batched.cuh"
+#include "coeffs.cuh"
 #include "pipe.cuh"
 #include "ws.cuh"
 #include "common.cuh"
@@ -93,9 +94,9 @@ __global__ void k_advance(LevelDev *descs, ThermalDev *tdescs, const DescMeta *m
   }
 }
 
-__global__ void k_tick(CaseDev *cases, int n_cases) {
+__global__ void k_tick(CaseDev *cases, int n_cases, int only_slot) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n_cases) cases[i].t += 1;
+  if (i < n_cases && (only_slot < 0 || i == only_slot)) cases[i].t += 1;
 }
 
 // Descriptor of the current work item, copied into shared memory by the CTA.
@@ -376,6 +377,8 @@ struct ol_ctx {
   // persistent kernel (cumulant without DDF; the other variants then take
   // one CTA per item)
   int grid_mult = -2;
+  // >= 0: the plan holds this case only (ol_ctx_case_step), -1: every case
+  int32_t only_case = -1;
   int64_t launches = 0;
   double *d_out = nullptr;
   std::mutex mu;
@@ -602,7 +605,8 @@ static void record_step(ol_ctx *c) {
       }
     }
   }
-  k_tick<<<(c->max_slots + 127) / 128, 128, 0, c->stream>>>(c->d_cases, c->max_slots);
+  const int only_slot = c->only_case >= 0 ? c->cases.at(c->only_case)->slot : -1;
+  k_tick<<<(c->max_slots + 127) / 128, 128, 0, c->stream>>>(c->d_cases, c->max_slots, only_slot);
 }
 
 // Build descriptors, work lists and the per-coarse-step graph.
@@ -611,7 +615,9 @@ static int rebuild(ol_ctx *c) {
   c->dirty = false;
   if (c->cases.empty()) return OL_OK;
   int lmax = 0;
-  for (auto &kv : c->cases) lmax = std::max<int>(lmax, (int)kv.second->levels.size());
+  for (auto &kv : c->cases)
+    if (c->only_case < 0 || kv.first == c->only_case)
+      lmax = std::max<int>(lmax, (int)kv.second->levels.size());
   std::vector<std::pair<int, int>> slots;  // (level, j)
   struct Walk {
     static void go(int l, int j, int lmax, std::vector<std::pair<int, int>> &out) {
@@ -643,6 +649,7 @@ static int rebuild(ol_ctx *c) {
     std::vector<WorkItem> ghost_items, tghost_items;
     for (auto &kv : c->cases) {
       NCase &cs = *kv.second;
+      if (c->only_case >= 0 && kv.first != c->only_case) continue;
       if ((int)cs.levels.size() < l) continue;
       const DevLevel &V = cs.levels[l - 1];
       const int d = (int)descs.size();
@@ -1103,6 +1110,42 @@ extern "C" int ol_ctx_step(ol_ctx *c, int32_t n) {
   return OL_OK;
 }
 
+extern "C" int ol_ctx_case_step(ol_ctx *c, int32_t id, int32_t n, float u_in) {
+  OL_CHECK_ARG(c && n >= 0, "ol_ctx_case_step: bad argument");
+  std::lock_guard<std::mutex> lk(c->mu);
+  auto it = c->cases.find(id);
+  if (it == c->cases.end()) return set_error(OL_ERR_STATE, "ol_ctx_case_step: unknown case %d", id);
+  OL_CUDA(cudaSetDevice(c->device));
+  NCase &cs = *it->second;
+  if (u_in >= 0.0f) {
+    // a fixed inlet speed from now on: no ramp
+    cs.u_target = u_in;
+    cs.ramp_steps = 0;
+    CaseDev *d = c->d_cases + cs.slot;
+    const int32_t zero = 0;
+    OL_CUDA(cudaMemcpyAsync(&d->u_target, &u_in, sizeof(float), cudaMemcpyHostToDevice, c->stream));
+    OL_CUDA(cudaMemcpyAsync(&d->ramp_steps, &zero, sizeof(int32_t), cudaMemcpyHostToDevice,
+                            c->stream));
+    OL_CUDA(cudaStreamSynchronize(c->stream));
+  }
+  if (n == 0) return OL_OK;
+  // a plan (and graph) of this case alone, replayed n times; the next
+  // ol_ctx_step rebuilds the plan of every resident case
+  c->only_case = id;
+  int rc = rebuild(c);
+  if (rc == OL_OK && c->exec)
+    for (int i = 0; i < n && rc == OL_OK; ++i) {
+      const cudaError_t e = cudaGraphLaunch(c->exec, c->stream);
+      if (e != cudaSuccess) rc = cuda_status(e, "cudaGraphLaunch");
+    }
+  c->only_case = -1;
+  c->dirty = true;
+  if (rc) return rc;
+  c->launches += c->launches_per_step * n;
+  cs.steps += n;
+  return OL_OK;
+}
+
 extern "C" int ol_ctx_step_timed(ol_ctx *c, int32_t n, float *ms) {
   OL_CHECK_ARG(c && ms && n >= 0, "ol_ctx_step_timed: bad argument");
   {
@@ -1176,6 +1219,16 @@ extern "C" int ol_ctx_case_forces(ol_ctx *c, int32_t id, double out[9]) {
   OL_LAUNCHED("ol_ctx_case_forces");
   OL_CUDA(cudaMemcpyAsync(out, dev_out, 9 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   OL_CUDA(cudaStreamSynchronize(c->stream));
+  return OL_OK;
+}
+
+extern "C" int ol_ctx_case_coefficients(ol_ctx *c, int32_t id, const ol_coeff_ref *ref,
+                                        double out[12]) {
+  OL_CHECK_ARG(c && ref && out, "ol_ctx_case_coefficients: null argument");
+  double raw[9];
+  const int rc = ol_ctx_case_forces(c, id, raw);
+  if (rc) return rc;
+  coefficients_from_sums(raw, ref, out);
   return OL_OK;
 }
 

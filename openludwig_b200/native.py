@@ -100,6 +100,16 @@ def coefficients(raw, rho_ref, u_ref, area_ref, chord_ref, symmetric=False) -> F
     return r
 
 
+def coeff_ref(case: PreparedCase) -> N.CoeffRef:
+    """Reference values of a case's force coefficients (surface.jl:873-910)."""
+    p = case.params
+    return N.CoeffRef(rho_ref=p.rho_physical, u_ref=p.u_physical, area_ref=p.reference_area,
+                      chord_ref=p.reference_chord, symmetric=int(bool(case.cfg.symmetric_analysis)))
+
+
+COEFF_NAMES = ("Cd", "Cl", "Cs", "Cmx", "Cmy", "Cmz", "Fx", "Fy", "Fz", "Mx", "My", "Mz")
+
+
 def force_params(case: PreparedCase, search_radius: int = 5) -> N.ForceParams:
     """map_surface_stresses! scalars (surface.jl:766-790) on the finest level."""
     p, cfg = case.params, case.cfg
@@ -253,6 +263,19 @@ class Context:
         p = case.params
         return coefficients(self.forces_raw(cid), p.rho_physical, p.u_physical, p.reference_area,
                             p.reference_chord, case.cfg.symmetric_analysis)
+
+    def coefficient_record(self, cid: int) -> dict:
+        """ol_ctx_case_coefficients: Cd, Cl, Cs, Cmx..z and the total forces
+        and moments of a case, computed by the library."""
+        out = (C.c_double * 12)()
+        ref = coeff_ref(self.cases[cid])
+        N.call("ol_ctx_case_coefficients", self._h, cid, C.byref(ref), out)
+        return dict(zip(COEFF_NAMES, out[:]))
+
+    def case_step(self, cid: int, n: int, u_in: float = -1.0) -> None:
+        """Advance one case alone (ol_ctx_case_step); u_in >= 0 fixes its
+        inlet speed from now on."""
+        N.call("ol_ctx_case_step", self._h, cid, n, u_in)
 
     def download(self, cid: int, level: int = 1, f: bool = False):
         h = self.cases[cid].levels[level - 1]

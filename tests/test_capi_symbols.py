@@ -29,7 +29,14 @@ def test_header_declares_entry_points():
     names = declared_symbols()
     for required in ("ol_stream_collide", "ol_bouzidi", "ol_bouzidi_sparse", "ol_thermal",
                      "ol_surface_forces", "ol_init_equilibrium", "ol_flow_stats",
-                     "ol_ctx_create", "ol_ctx_step", "ol_last_error"):
+                     "ol_ctx_create", "ol_ctx_step", "ol_last_error",
+                     # per-case control and the coefficient record
+                     "ol_ctx_case_step", "ol_ctx_case_coefficients",
+                     # serving through the C ABI
+                     "ol_server_create", "ol_serve_submit", "ol_serve_advance", "ol_serve_poll",
+                     "ol_serve_history", "ol_server_destroy",
+                     # kernel and launch-shape control
+                     "ol_set_stream_collide_kernel", "ol_ctx_set_launch", "ol_pipeline_fault"):
         assert required in names
 
 
@@ -54,6 +61,13 @@ def test_argument_errors_are_reported_not_raised(lib):
     assert b"null" in lib.ol_last_error()
     lib.ol_ctx_create.restype = ctypes.c_int
     assert lib.ol_ctx_create(None, 0, ctypes.c_size_t(1 << 20), 0) == 1
+    # serving and per-case entry points check their arguments first too
+    assert lib.ol_server_create(None, None, None) == 1
+    assert lib.ol_serve_submit(None, None, None, ctypes.c_double(0.0), None) == 1
+    assert lib.ol_serve_advance(None, None, None) == 1
+    assert lib.ol_ctx_case_step(None, 0, 1, ctypes.c_float(-1.0)) == 1
+    assert lib.ol_ctx_case_coefficients(None, 0, None, None) == 1
+    assert lib.ol_set_stream_collide_kernel(7, 0) == 1
 
 
 def test_ctypes_struct_layouts_match_header(tmp_path):
@@ -71,7 +85,9 @@ def test_ctypes_struct_layouts_match_header(tmp_path):
              "ol_parent_view": N.ParentView, "ol_thermal_view": N.ThermalView,
              "ol_surface_mesh": N.SurfaceMesh, "ol_restrict_view": N.RestrictView,
              "ol_net_force_maps": N.NetForceMaps, "ol_output_level": N.OutputLevel,
-             "ol_output_fields": N.OutputFields, "ol_bouzidi_link": N.BouzidiLink}
+             "ol_output_fields": N.OutputFields, "ol_bouzidi_link": N.BouzidiLink,
+             "ol_coeff_ref": N.CoeffRef, "ol_serve_rule": N.ServeRule,
+             "ol_serve_result": N.ServeResult}
     src = tmp_path / "sizes.c"
     src.write_text('#include <stdio.h>\n#include "openludwig_b200.h"\nint main(void){\n' +
                    "".join(f'printf("%zu\\n", sizeof({n}));\n' for n in names) + "return 0;}\n")

@@ -1,7 +1,9 @@
-"""Continuous-batching service: requests that arrive while others run are
-admitted as memory frees up, and every result equals the same request run
-alone (bitwise: each case's kernels only read its own state, and its force
-sums are fixed-order FP64)."""
+"""Continuous-batching service through the library's serving layer
+(ol_server_* / ol_serve_*, driven by serving.Server): requests that arrive
+while others run are admitted as memory frees up, and every result equals
+the same request run alone (bitwise: each case's kernels only read its own
+state, and its force sums are fixed-order FP64).  Per-case control through
+the C ABI: ol_ctx_case_step and the coefficient record."""
 import numpy as np
 import pytest
 
@@ -60,3 +62,66 @@ def test_admission_waits_for_memory():
     admits = sorted(r.admit_s for r in out["results"])
     assert admits[-1] > admits[0]      # later requests waited for a retirement
     assert all(np.isfinite(r.cd) for r in out["results"])
+
+
+def test_lazy_requests_count_their_preparation():
+    """A request given as a preparation function is prepared on arrival, and
+    its latency includes that preparation."""
+    a = _case(8)
+
+    def make():
+        import time
+        time.sleep(0.2)
+        return a
+
+    ctx = NT.Context(budget_bytes=1 << 30, storage="f16")
+    out = SV.Server(ctx, check_every=10, window=20, tol=1e-9, max_steps=20).run(
+        [SV.Request(0, 0.0, make)])
+    ctx.close()
+    r = out["results"][0]
+    assert r.prep_s >= 0.2 and r.latency_s >= r.prep_s and r.steps == 20
+
+
+def test_case_step_moves_one_case_and_matches_alone():
+    """ol_ctx_case_step advances one resident case only; its state is the
+    state of the case stepped alone, and u_in fixes its inlet speed the same
+    way in a mix as alone."""
+    a = _case(8)
+    b = _case(16, 2)
+    ctx = NT.Context(budget_bytes=1 << 30, storage="f32")
+    ca, cb = ctx.add_case(a), ctx.add_case(b)
+    ctx.case_step(ca, 5)
+    assert ctx.info(ca)[0] == 5 and ctx.info(cb)[0] == 0
+    fa = ctx.download(ca, 1, f=True)[2]
+    ctx.step(2)                                   # the full plan again: both move
+    assert ctx.info(ca)[0] == 7 and ctx.info(cb)[0] == 2
+    ctx.case_step(cb, 3, u_in=0.03)
+    assert ctx.info(cb)[0] == 5 and ctx.info(ca)[0] == 7
+    fb = ctx.download(cb, 2, f=True)[2]
+    ctx.close()
+    alone = NT.Context(budget_bytes=1 << 30, storage="f32")
+    ia = alone.add_case(a)
+    alone.step(5)
+    assert np.array_equal(alone.download(ia, 1, f=True)[2], fa)
+    alone.close()
+    ref = NT.Context(budget_bytes=1 << 30, storage="f32")
+    ib = ref.add_case(b)
+    ref.step(2)
+    ref.case_step(ib, 3, u_in=0.03)
+    assert np.array_equal(ref.download(ib, 2, f=True)[2], fb)
+    ref.close()
+
+
+def test_coefficient_record_matches_the_raw_sums():
+    a = _case(8)
+    ctx = NT.Context(budget_bytes=1 << 30, storage="f32")
+    cid = ctx.add_case(a)
+    ctx.step(20)
+    rec = ctx.coefficient_record(cid)
+    raw = ctx.forces_raw(cid)
+    fr = ctx.forces(cid)
+    ctx.close()
+    assert rec["Cd"] == fr.Cd and rec["Cl"] == fr.Cl and rec["Cs"] == fr.Cs
+    assert rec["Cmy"] == fr.Cmy
+    assert rec["Fx"] == raw[0] + raw[3] and rec["Mz"] == raw[8]
+    assert rec["Cd"] != 0.0
