@@ -21,10 +21,24 @@ Reported:
               statistics) read back to pinned host memory every step
   roofline    HBM roofline of the dominant kernel (finest-level stream-collide)
               from CUDA events around repeated launches of it
+  mlups_reference_formula  the reference's own figure (main.jl:232): active
+              cells of all levels once per coarse step / time, beside the
+              sub-step-weighted value
+  batched     the block pool on config 4 (48 seeded uneven cases in one pool):
+              FP16-shifted and FP32 MLUPS, HBM roofline fraction at 108 / 216
+              bytes per update, drag error of FP16 storage against the FP64
+              oracle on a probe case
+  served      continuous batching on a sample of the config-5 stream (the
+              config-4 mix plus 10 % large cases, Poisson arrivals at 80 % of
+              the measured capacity, 2000-step window, 160 GB budget), with
+              case preparation inside each request's latency, against the same
+              requests solved one at a time on the plain FP32 drop-in path
   cpu_baseline the CPU oracle (restatement of the reference's algorithm) on the
               host cores, over a bounded number of coarse steps
 Multi-GPU: one independent replica per rank (the reference has no multi-GPU
 path; cases shard by case), scaling "weak", value = sum over ranks / max time.
+`--gpus N` without torchrun starts the N ranks itself (torch.distributed.run
+on 127.0.0.1).
 """
 from __future__ import annotations
 
@@ -193,14 +207,50 @@ def launches_per_coarse_step(levels, ddf: bool) -> int:
     return total
 
 
-def describe(workload, p, hosts) -> dict:
+def describe(workload, p, hosts, world: int = 1) -> dict:
+    """The `config` of the JSON line, identical in both arms."""
     return {"workload": workload, "levels": len(hosts),
             "coarse_domain": [p.nx_coarse, p.ny_coarse, p.nz_coarse],
             "blocks_per_level": [h.n_blocks for h in hosts],
             "cells": int(sum(h.n_blocks * 512 for h in hosts)),
             "cell_updates_per_step": int(sum(h.n_blocks * 512 * (1 << i) for i, h in enumerate(hosts))),
             "boundary_cells": int(sum(h.n_boundary for h in hosts)),
-            "l2_policy": "state larger than L2 (no flush needed)"}
+            "l2_policy": "state larger than L2 (no flush needed)",
+            "parallelism": f"replicas x{world}", "storage": "f32",
+            "step": "one coarse step (recursive 2:1 sequence)"}
+
+
+def relaunch_under_torchrun(gpus: int) -> None:
+    """`--gpus N` run directly: start N local ranks through
+    torch.distributed.run (rendezvous on 127.0.0.1) and exit with its status."""
+    import socket
+    with socket.socket() as so:
+        so.bind(("127.0.0.1", 0))
+        port = so.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1",
+           f"--nproc-per-node={gpus}", "--master-addr", "127.0.0.1", "--master-port", str(port),
+           os.path.abspath(__file__)] + sys.argv[1:]
+    raise SystemExit(subprocess.call(cmd))
+
+
+def launcher_selftest(a, rank: int, world: int) -> None:
+    """The multi-rank plumbing without a GPU (gloo): barrier, a max over the
+    ranks' elapsed times, one line from rank 0 with n_gpus = world."""
+    import torch
+    import torch.distributed as dist
+    if world > 1:
+        dist.init_process_group("gloo", timeout=__import__("datetime").timedelta(seconds=60))
+    t = torch.tensor([0.5 + rank], dtype=torch.float64)
+    if world > 1:
+        dist.barrier()
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    if rank == 0:
+        print(json.dumps({"metric": "MLUPS", "value": None, "n_gpus": world, "selftest": True,
+                          "max_rank_ms": float(t.item()), "steps": a.steps,
+                          "warmup": a.warmup}), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
 
 
 def time_cpu_baseline(cfg, p, hosts, budget_s: float = 15.0) -> dict:
@@ -224,6 +274,112 @@ def time_cpu_baseline(cfg, p, hosts, budget_s: float = 15.0) -> dict:
             "sample": f"{n} coarse step(s) of the workload, FP32 oracle, OpenMP over blocks"}
 
 
+def accuracy_probe(dev) -> dict:
+    """Drag of FP16-shifted pool storage against the FP64 oracle on a small
+    sphere case (64x32x32, 100 steps, same surface-force integration)."""
+    from oracle import driver as odrv
+    from oracle import oracle as orc
+    from openludwig_b200 import domain, native as NT, scaling, solver as S, workloads
+    orc.build()
+    cfg, mesh = workloads.sphere_1lvl(8)
+    p = scaling.compute_domain_from_mesh(cfg, mesh.min_bounds, mesh.max_bounds)
+    hosts = domain.setup_multilevel_domain(cfg, mesh, p)
+    steps = 100
+    st = S.StepSettings.from_config(cfg, False)
+    case = NT.PreparedCase(cfg, mesh, p, hosts, st)
+    ctx = NT.Context(budget_bytes=1 << 30, storage="f16")
+    cid = ctx.add_case(case)
+    ctx.step(steps)
+    c16 = ctx.forces(cid)
+    ctx.close()
+    o = odrv.init_levels(hosts, dtype=np.float64)
+    s = odrv.settings_dict(st)
+    dims = (p.nx_coarse, p.ny_coarse, p.nz_coarse)
+    for t in range(1, steps + 1):
+        odrv.recursive_step(o, s, 0, t, None, 0.0, float(cfg.u_target), dims, np.float64)
+    lv = S.upload_level(hosts[0], dev)
+    dmesh = S.upload_mesh(mesh, dev)
+    raw64, _ = orc.surface_forces(dmesh.arrays.cpu().numpy(), o[0].rho.astype(np.float32),
+                                  o[0].vel.astype(np.float32), lv.obstacle.cpu().numpy(),
+                                  lv.block_ptr.cpu().numpy(), lv.n_blocks,
+                                  S.force_params_for(lv, p, cfg))
+    c64 = NT.coefficients(raw64, p.rho_physical, p.u_physical, p.reference_area, p.reference_chord)
+    return {"value": abs(c16.Cd / c64.Cd - 1), "Cl_abs_over_Cd": abs(c16.Cl - c64.Cl) / abs(c64.Cd),
+            "sample": "64x32x32 sphere, 100 steps: FP16-shifted pool vs the FP64 oracle"}
+
+
+def bench_batched(a, dev, local, peak_gbs, plain_value) -> dict:
+    """Config 4: 48 seeded uneven cases in one pool, FP16-shifted and FP32."""
+    from openludwig_b200 import native as NT
+    from openludwig_b200.serve_bench import case_makers
+    t0 = time.perf_counter()
+    cases = [mk() for mk in case_makers(48, 1234, local)]
+    prep_s = time.perf_counter() - t0
+    upd = sum(c.cell_updates_per_step for c in cases)
+    out = {"cases": len(cases), "seed": 1234, "cell_updates_per_step": int(upd),
+           "prep_s": prep_s, "workload": "batch_mix 48 (sphere / cube / NACA0012 wing, "
+           "16-48 finest cells, 1-3 levels, Re 1e3-1e6), cumulant + WALE"}
+    for storage in ("f16", "f32"):
+        probe = NT.Context(device=local, budget_bytes=64 << 20, storage=storage)
+        need = sum(probe.footprint(c) for c in cases)
+        probe.close()
+        ctx = NT.Context(device=local, budget_bytes=int(need * 1.2) + (256 << 20), storage=storage)
+        for c in cases:
+            ctx.add_case(c)
+        ctx.step(a.warmup)
+        ctx.sync()
+        k = max(4, a.steps)
+        ms = ctx.step_timed(k)
+        mlups = upd * k / (ms / 1e3) / 1e6
+        gbs = mlups * 1e6 * B_ALG[storage] / 1e9
+        out[storage] = {"MLUPS": mlups, "ms_per_step": ms / k, "roofline_achieved_GBs": gbs,
+                        "roofline_frac": gbs / peak_gbs, "bytes_per_cell_update_alg": B_ALG[storage],
+                        "launch": ctx.launch()}
+        ctx.close()
+    out["f16_over_f32_batched"] = out["f16"]["MLUPS"] / out["f32"]["MLUPS"]
+    out["f16_over_f32_plain"] = out["f16"]["MLUPS"] / plain_value
+    out["cd_err_vs_fp64"] = accuracy_probe(dev)
+    return out
+
+
+def bench_served(a, dev, local, batched) -> dict:
+    """A sample of config 5: the config-4 mix plus 10 % large cases, prepared
+    on arrival; closed loop (all at t = 0) gives the capacity; then Poisson
+    arrivals at 80 % of it; the same requests one at a time on the plain FP32
+    drop-in path with the same arrivals."""
+    import torch
+    from openludwig_b200 import native as NT
+    from openludwig_b200 import serving as SV
+    from openludwig_b200.serve_bench import case_makers, summary
+    n = a.served_requests
+    rule = dict(check_every=200, window=2000, tol=1e-3, max_steps=10000)
+    budget = min(160 << 30, int(torch.cuda.mem_get_info(dev)[0] * 0.85))
+    makers = case_makers(n, 4321, local, large_frac=0.1)
+    out = {"requests": n, "config5_requests": 500, "seed": 4321, "large_frac": 0.1,
+           "rule": rule, "budget_bytes": budget, "storage": "f16",
+           "note": (f"a {n}-request sample of the config-5 stream (500 requests do not fit the "
+                    "bench's time); latency counts case preparation")}
+    ctx = NT.Context(device=local, budget_bytes=budget, storage="f16")
+    closed = SV.Server(ctx, **rule).run([SV.Request(i, 0.0, mk) for i, mk in enumerate(makers)])
+    ctx.close()
+    rate = 0.8 * closed["solves_per_hour"] / 3600.0
+    arrivals = SV.poisson_arrivals(n, rate, seed=4321)
+    ctx = NT.Context(device=local, budget_bytes=budget, storage="f16")
+    opened = SV.Server(ctx, **rule).run([SV.Request(i, float(arrivals[i]), mk)
+                                          for i, mk in enumerate(makers)])
+    ctx.close()
+    serial = SV.serial_baseline(makers, arrivals, **rule, device=dev)
+    out["capacity_closed_loop"] = summary(closed)
+    out["poisson_rate_per_s"] = rate
+    out["served"] = summary(opened)
+    out["serial_f32_dropin"] = summary(serial)
+    out["solves_per_hour"] = opened["solves_per_hour"]
+    out["p50_s"], out["p99_s"] = opened["p50_s"], opened["p99_s"]
+    out["served_over_serial"] = opened["solves_per_hour"] / serial["solves_per_hour"]
+    out["cd_err_vs_fp64"] = batched.get("cd_err_vs_fp64")
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -234,12 +390,24 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--clocks-dir", default=None,
                     help="also write the clock samples of the timed region to this directory")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the batched and served blocks")
+    ap.add_argument("--served-requests", type=int, default=24,
+                    help="requests of the served sample (config 5 asks for 500)")
+    ap.add_argument("--launcher-selftest", action="store_true", help=argparse.SUPPRESS)
     a = ap.parse_args()
     a.warmup = max(a.warmup, 3)
 
+    if a.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        relaunch_under_torchrun(a.gpus)
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world != a.gpus:
+        raise SystemExit(f"bench.py: --gpus {a.gpus} but the launcher started {world} rank(s)")
+    if a.launcher_selftest:
+        launcher_selftest(a, rank, world)
+        return
 
     if a.impl == "reference":
         if rank != 0:
@@ -264,11 +432,13 @@ def main():
             odrv.recursive_step(lv, s, 0, t, None, 0.0, float(cfg.u_target), dims, np.float32)
         dt = time.perf_counter() - t0
         v = upd * k / dt / 1e6
+        cells = sum(h.n_blocks * 512 for h in hosts)
         line = {"impl": "reference", "metric": "MLUPS", "value": v, "unit": "MLUPS",
                 "n_gpus": a.gpus, "device": "cpu",
                 "steps": k, "warmup": a.warmup, "ms_per_step": dt / k * 1e3, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-                "config": describe(a.workload, p, hosts),
+                "config": describe(a.workload, p, hosts, a.gpus),
+                "mlups_reference_formula": cells * k / dt / 1e6,
                 "cpu_baseline": {"value": v, "unit": "MLUPS", "cores": os.cpu_count(), "kind": "port",
                                  "sample": f"{k} coarse step(s) of the workload after {a.warmup} "
                                            "warm-up step(s), FP32 oracle, OpenMP over blocks"},
@@ -474,13 +644,20 @@ def main():
             cpu = {"value": None, "unit": "MLUPS", "cores": os.cpu_count(), "kind": "port",
                    "sample": f"unavailable: {ex}"}
 
+    extras = {}
+    if rank == 0 and world == 1 and not a.no_extras:
+        peak_gbs = peaks()[0]
+        extras["batched"] = bench_batched(a, dev, local, peak_gbs, value)
+        extras["served"] = bench_served(a, dev, local, extras["batched"])
+
     if rank == 0:
+        cells = sum(h.n_blocks * 512 for h in hosts)
         line = {
             "metric": "MLUPS", "value": value, "unit": "MLUPS", "n_gpus": world, "steps": nsteps,
             "warmup": a.warmup, "ms_per_step": dt_ms / nsteps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": dict(describe(a.workload, p, hosts), parallelism=f"replicas x{world}",
-                           storage="f32", step="one coarse step (recursive 2:1 sequence)"),
+            "config": describe(a.workload, p, hosts, world),
+            "mlups_reference_formula": value * cells / upd,
             "e2e": {"value": e2e, "unit": "MLUPS", "h2d_bytes_per_step": h2d_per_step,
                     "d2h_bytes_per_step": 7 * 8},
             "gpu_launches": launches_per_step * nsteps,
@@ -493,6 +670,7 @@ def main():
                          "alg_bytes_per_launch": alg_bytes, "avg_launch_ms": k_ms},
             "clocks": clocks,
             "native": native,
+            **extras,
             "cpu_baseline": cpu,
         }
         print(json.dumps(line), flush=True)

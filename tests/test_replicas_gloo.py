@@ -50,3 +50,25 @@ def test_single_process_is_identity():
     assert replicas.world() == (0, 1)
     rate, ms = replicas.job_rate(5e6, 25.0)
     assert ms == 25.0 and rate == pytest.approx(2e8)
+
+
+def test_bench_gpus_flag_starts_the_ranks_itself():
+    """`python bench.py --gpus 2` without torchrun starts two ranks (here its
+    CPU self-test of the launcher: gloo barrier and max over ranks) and
+    reports n_gpus = 2 from rank 0."""
+    import json
+    import os
+    import subprocess
+    import sys
+    from pathlib import Path
+    root = Path(__file__).resolve().parent.parent
+    env = {k: v for k, v in os.environ.items()
+           if k not in ("RANK", "WORLD_SIZE", "LOCAL_RANK", "MASTER_ADDR", "MASTER_PORT")}
+    r = subprocess.run([sys.executable, str(root / "bench.py"), "--gpus", "2", "--steps", "2",
+                        "--warmup", "3", "--launcher-selftest"], capture_output=True, text=True,
+                       timeout=300, env=env, cwd=str(root))
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [json.loads(x) for x in r.stdout.splitlines() if x.startswith("{")]
+    assert len(lines) == 1
+    assert lines[0]["n_gpus"] == 2 and lines[0]["selftest"]
+    assert lines[0]["max_rank_ms"] == 1.5      # the slower rank's time wins
