@@ -605,7 +605,7 @@ def main():
     # DRAM bytes per call of the same finest-level launch, from the committed
     # ncu summary of this workload (null when there is none)
     traffic = None
-    prof = os.path.join(ROOT, "profiles", f"k_stream_collide_{a.workload}_level{len(levels)}.md")
+    prof = os.path.join(ROOT, "profiles", f"k_sc_ws_{a.workload}_level{len(levels)}.md")
     if os.path.exists(prof):
         with open(prof) as fh:
             m = re.search(r"^traffic_bytes_per_launch\s*=\s*(\d+)", fh.read(), re.M)
@@ -664,7 +664,7 @@ def main():
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
                          "kernel": "ol_stream_collide on the finest level (k_ghost_fill + "
-                                   "k_stream_collide), mean over the pair of sub-steps per "
+                                   "k_sc_ws), mean over the pair of sub-steps per "
                                    "parent step",
                          "peak_source": peak_kind,
                          "alg_bytes_per_launch": alg_bytes, "avg_launch_ms": k_ms},
