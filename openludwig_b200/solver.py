@@ -435,8 +435,52 @@ def execute_timestep_batch(levels, s: StepSettings, t_start: int, batch: int, u:
         recursive_step(levels, s, 0, t_start + off, None, 0.0, u, domain_dims)
 
 
+@dc.dataclass
+class Batch:
+    """One pass of main.jl's time loop (main.jl:212-313): steps t..end at one
+    inlet velocity u; diag_step / out_step are the diagnostics and output
+    steps that fall inside the batch (None when none does)."""
+    t: int
+    end: int
+    actual: int
+    u: float
+    diag_step: int | None
+    out_step: int | None
+
+
+def main_loop_batches(first: int, last: int, async_depth: int, diag_freq: int,
+                      output_freq: int, ramp_steps: int, u_target: float):
+    """main.jl:212-313 schedule: batches of async_depth steps, the inlet
+    velocity of a batch evaluated at its end step; a diagnostics step is
+    the multiple of diag_freq that the batch crosses (also checked on the
+    run's last batch); an output step likewise for output_freq."""
+    batch = max(1, async_depth)
+    of = max(1, output_freq)
+    t = first
+    while t <= last:
+        end = min(t + batch - 1, last)
+        actual = end - t + 1
+        diag = out = None
+        if end % diag_freq < actual or end == last:
+            d = (end // diag_freq) * diag_freq
+            if t <= d <= end:
+                diag = d
+        if end % of < actual:
+            o = (end // of) * of
+            if t <= o <= end:
+                out = o
+        yield Batch(t, end, actual, ramp_velocity(u_target, end, ramp_steps), diag, out)
+        t = end + 1
+
+
 def ramp_velocity(u_target: float, batch_end: int, ramp_steps: int) -> float:
-    """main.jl:217-218: cosine ramp evaluated once per batch at its end step."""
+    """main.jl:217-218: cosine ramp evaluated once per batch at its end step,
+    in Float32: prog = 0.5f0 (1 - cos(Float32(pi) batch_end / ramp)).  The
+    Float32 argument is formed as Julia forms it (Float32 product, then
+    Float32 quotient); cos is taken in double and rounded once to Float32,
+    which is how Julia's cos(::Float32) works too (Float64 kernel, one
+    rounding), so the two agree except where cos lies within that kernel's
+    error of a Float32 rounding midpoint (then by one ulp of u)."""
     if ramp_steps > 0 and batch_end <= ramp_steps:
         prog = np.float32(0.5) * (np.float32(1.0) - np.float32(math.cos(np.float32(math.pi) * batch_end / ramp_steps)))
     else:
@@ -544,12 +588,19 @@ def flow_stats(lv: DeviceLevel) -> dict:
 class Simulation:
     """main.jl solve_main() time loop over the device levels: batched cosine
     inlet ramp, diagnostics every diag_freq steps, surface forces on the
-    finest level, time averaging after the ramp (ForceAccumulator)."""
+    finest level, time averaging after the ramp (ForceAccumulator), and,
+    with an output folder, the files the reference writes there.
 
-    def __init__(self, cfg: CaseConfig, mesh, p: DomainParams, hosts, device=None):
+    `unrotated_mesh` is the body in its STL frame (before the angle-of-attack
+    rotation); the surface-pressure and net-force files use it as the
+    reference does (main.jl:281-304).  Without it they use `mesh`."""
+
+    def __init__(self, cfg: CaseConfig, mesh, p: DomainParams, hosts, device=None,
+                 unrotated_mesh=None):
         from .native import coefficients
         self._coeff = coefficients
         self.cfg, self.mesh, self.p = cfg, mesh, p
+        self.unrotated_mesh = unrotated_mesh if unrotated_mesh is not None else mesh
         self.device = device or torch.device("cuda", torch.cuda.current_device())
         self.levels = [upload_level(h, self.device, ddf=cfg.ddf_enabled, t_init=cfg.ddf_t_initial)
                        for h in hosts]
@@ -560,56 +611,114 @@ class Simulation:
         self.history: list[dict] = []
         self.acc = np.zeros(9)
         self.n_avg = 0
+        self._records = None
+        self._out = None
 
-    def forces(self):
-        raw = compute_aerodynamics(self.levels[-1], self.dmesh, self.p, self.cfg)
-        return self._coeff(raw, self.p.rho_physical, self.p.u_physical, self.p.reference_area,
-                           self.p.reference_chord, self.cfg.symmetric_analysis), raw
+    def forces(self, maps: bool = False):
+        got = compute_aerodynamics(self.levels[-1], self.dmesh, self.p, self.cfg, maps=maps)
+        raw, m = got if maps else (got, None)
+        fr = self._coeff(raw, self.p.rho_physical, self.p.u_physical, self.p.reference_area,
+                         self.p.reference_chord, self.cfg.symmetric_analysis)
+        return (fr, raw, m) if maps else (fr, raw)
+
+    def _sample(self, step: int, maps: bool):
+        """compute_aerodynamics! + accumulate_forces! after the ramp."""
+        fr, raw, m = self.forces(maps=True) if maps else (*self.forces(), None)
+        if step > self.cfg.ramp_steps:
+            self.acc += raw
+            self.n_avg += 1
+        return fr, m
 
     def run(self, steps: int, diag_freq: int | None = None,
             output_dir: str | None = None) -> list[dict]:
-        """With output_dir, the merged flow field is exported every
-        cfg.output_freq steps (main.jl:259-263, io_vtk.jl) as
-        flow_%06d.vtu: gathered on the device at the batch end that crosses
-        the output step, copied back while the next batches run, and written
-        at the next output or at the end of run()."""
+        """Advance `steps` steps in main.jl's batches (main_loop_batches).
+        At a diagnostics step: flow statistics of level 1, forces on the
+        finest level (accumulated after the ramp).  At an output step that is
+        not a diagnostics multiple the forces are sampled and accumulated as
+        well (main.jl:267-275).  With output_dir: convergence.csv and
+        forces.csv rows per diagnostics step; per output step the merged
+        flow field flow_%06d.vtu (gathered on the device at the batch end,
+        copied back while the next batches run, written at the next output
+        or at the end), surface_%06d.lbmp and, with net-force export,
+        net_forces_%06d.csv; and a final output at the run's last step when
+        that is not an output step (main.jl:316-360)."""
+        import time as _time
         cfg = self.cfg
         diag = diag_freq or cfg.diag_freq
-        batch = max(1, cfg.async_depth)
-        end = self.t + steps
-        t = self.t + 1
+        last = self.t + steps
         pending = None
-        if output_dir is not None and getattr(self, "_out", None) is None:
+        fwd = cfg.forces_enabled
+        if output_dir is not None:
             from .output import MergedOutput
-            self._out = MergedOutput(self.levels)
-        while t <= end:
-            batch_end = min(t + batch - 1, end)
-            actual = batch_end - t + 1
-            u = ramp_velocity(cfg.u_target, batch_end, cfg.ramp_steps)
-            execute_timestep_batch(self.levels, self.settings, t, actual, u, self.dims)
-            of = max(1, cfg.output_freq)
-            if output_dir is not None and batch_end % of < actual:
-                out_step = (batch_end // of) * of
-                if t <= out_step <= batch_end:
+            if self._out is None:
+                self._out = MergedOutput(self.levels)
+            if self._records is None:
+                from .records import RunRecords
+                self._records = RunRecords(output_dir, fwd)
+        cells = cells_total(self.levels)
+        last_diag = _time.perf_counter()
+        maps = None
+        for b in main_loop_batches(self.t + 1, last, cfg.async_depth, diag, cfg.output_freq,
+                                   cfg.ramp_steps, cfg.u_target):
+            execute_timestep_batch(self.levels, self.settings, b.t, b.actual, b.u, self.dims)
+            want_maps = output_dir is not None and b.out_step is not None
+            if b.diag_step is not None:
+                d = b.diag_step
+                rec = {"step": d, "u": b.u, **flow_stats(self.levels[0])}
+                fr = None
+                if fwd:
+                    fr, maps = self._sample(d, want_maps)
+                    rec.update(Cd=fr.Cd, Cl=fr.Cl, Cs=fr.Cs, Cmy=fr.Cmy)
+                self.history.append(rec)
+                if self._records is not None and output_dir is not None:
+                    now = _time.perf_counter()
+                    mlups = cells * diag / ((now - last_diag) * 1e6)
+                    last_diag = now
+                    tp = float(d) * self.p.time_scale
+                    lx = self.p.domain_size[0]
+                    travel = 100.0 * (tp * self.p.u_physical) / lx if lx > 0 else 0.0
+                    self._records.append(d, tp, travel, b.u, rec["rho_min"], mlups, fr)
+            if b.out_step is not None:
+                o = b.out_step
+                if fwd and o != (o // diag) * diag:
+                    _, maps = self._sample(o, want_maps)
+                if output_dir is not None:
                     if pending is not None:
                         self._write(output_dir, pending)
-                    pending = self._out.pack(out_step)
-            if batch_end % diag < actual or batch_end == end:
-                d = (batch_end // diag) * diag
-                if t <= d <= batch_end:
-                    rec = {"step": d, "u": u, **flow_stats(self.levels[0])}
-                    if cfg.forces_enabled:
-                        fr, raw = self.forces()
-                        rec.update(Cd=fr.Cd, Cl=fr.Cl, Cs=fr.Cs, Cmy=fr.Cmy)
-                        if d > cfg.ramp_steps:
-                            self.acc += raw
-                            self.n_avg += 1
-                    self.history.append(rec)
-            t = batch_end + 1
-        self.t = end
+                    pending = self._out.pack(o)
+                    if fwd:
+                        self._surface_files(output_dir, o, maps)
+        self.t = last
+        if output_dir is not None:
+            of = max(1, cfg.output_freq)
+            if (last // of) * of != last or last < of:
+                if pending is not None:
+                    self._write(output_dir, pending)
+                pending = self._out.pack(last)
+                if fwd:
+                    _, _, maps = self.forces(maps=True)
+                    self._surface_files(output_dir, last, maps)
         if pending is not None:
             self._write(output_dir, pending)
         return self.history
+
+    def _surface_files(self, output_dir: str, step: int, maps) -> None:
+        """surface_%06d.lbmp from the pressure / shear maps of the last force
+        evaluation, in the STL frame without domain offset (main.jl:284-287);
+        net_forces_%06d.csv when net-force export is on (main.jl:290-301)."""
+        import os
+        from .records import write_net_forces_csv, write_surface_pressure_bin
+        m = maps.cpu().numpy()
+        um = self.unrotated_mesh
+        write_surface_pressure_bin(os.path.join(output_dir, "surface_%06d.lbmp" % step),
+                                   um.triangles, um.normals, m[0], m[1:4],
+                                   self.p.rho_physical, self.p.u_physical)
+        if self.cfg.net_force_export:
+            net = compute_net_aerodynamics(self.levels[-1], self.dmesh, self.p, self.cfg)
+            write_net_forces_csv(os.path.join(output_dir, "net_forces_%06d.csv" % step),
+                                 np.stack(net), self.mesh.centers, self.p.mesh_offset,
+                                 unrotated_centers=self.unrotated_mesh.centers,
+                                 alpha_deg=self.cfg.alpha_deg, beta_deg=self.cfg.beta_deg)
 
     @staticmethod
     def _write(output_dir: str, snap) -> None:

@@ -508,4 +508,126 @@ int orc_bouzidi_qmap(const int32_t *coords, int n, const double *tris, int ntri,
 
 uint16_t orc_double_to_half(double x) { return d2h(x); }
 
+/* Case scaling (physics_scaling.jl:63-191, compute_domain_from_mesh), FP64 in
+ * the reference's expression order.  Inputs are the configuration globals
+ * the reference reads (config_loader.jl); u_lattice and tau_min arrive as
+ * the Float32 values the loader stores. */
+struct OrcScaleIn {
+  double mesh_min[3], mesh_max[3];
+  double ref_length_cfg;   // REFERENCE_LENGTH_FOR_MESHING (<= 0: from the mesh)
+  int32_t ref_dim;         // 0 :x, 1 :y, 2 :z, other: maximum extent
+  double ref_chord_cfg, ref_area_cfg;
+  int32_t symmetric;
+  double moment_center[3];
+  double u_phys, nu_phys, rho_phys;
+  int32_t surface_resolution;
+  float u_lattice, tau_min;
+  double upstream, downstream, lateral, height;
+  int32_t block_size, min_coarse_blocks, num_levels_cfg, auto_levels, max_levels;
+  int32_t ddf_enabled;
+  double prandtl;
+};
+
+struct OrcScaleOut {
+  int32_t num_levels, nx, ny, nz, bx, by, bz;
+  double ref_length, ref_chord, ref_area, re, tau_fine;
+  double domain[3], offset[3], moment_center[3];
+  double dx_fine, dx_coarse, dx_levels[16];
+  double length_scale, velocity_scale, time_scale, nu_lattice, force_scale;
+  float tau_levels[16];
+  double tau_g_fine;
+  float tau_g_levels[16];
+};
+
+int orc_domain_scaling(const OrcScaleIn *in, OrcScaleOut *o) {
+  std::memset(o, 0, sizeof(*o));
+  const double *mn = in->mesh_min, *mx = in->mesh_max;
+  double ctr[3], ext[3];
+  for (int i = 0; i < 3; ++i) {
+    ctr[i] = (mn[i] + mx[i]) / 2;
+    ext[i] = mx[i] - mn[i];
+  }
+  double L;
+  if (in->ref_length_cfg > 0) L = in->ref_length_cfg;
+  else if (in->ref_dim == 0) L = ext[0];
+  else if (in->ref_dim == 1) L = ext[1];
+  else if (in->ref_dim == 2) L = ext[2];
+  else L = std::max(ext[0], std::max(ext[1], ext[2]));
+  o->ref_length = L;
+  o->ref_chord = in->ref_chord_cfg > 0 ? in->ref_chord_cfg : ext[0];
+  o->ref_area = in->ref_area_cfg > 0 ? in->ref_area_cfg
+                                     : (in->symmetric ? ext[1] * ext[2] * 2 : ext[1] * ext[2]);
+  const double re = in->u_phys * L / in->nu_phys;
+  o->re = re;
+  // compute_tau_for_levels (:63-66): nu = Float64(u_lattice) * N / Re; tau = 3 nu + 1/2
+  const double nu_f = (double)in->u_lattice * in->surface_resolution / re;
+  const double tau_c = 3.0 * nu_f + 0.5;
+  const double tau_fine = std::max(tau_c, (double)in->tau_min);
+  o->tau_fine = tau_fine;
+  double dx = L * (in->upstream + in->downstream) + ext[0];
+  double dy = in->symmetric ? (mx[1] + L * in->lateral) : (ext[1] + 2 * L * in->lateral);
+  double dz = ext[2] + 2 * L * in->height;
+  const double dx_fine = L / in->surface_resolution;
+  // compute_max_levels_for_domain (:68-71)
+  const double ratio = std::min(dx, std::min(dy, dz)) / (dx_fine * in->min_coarse_blocks * in->block_size);
+  const int max_lv = ratio < 1.0 ? 1 : (int)std::floor(1 + std::log2(ratio));
+  int nl;
+  if (in->num_levels_cfg > 0) nl = std::min(in->num_levels_cfg, max_lv);
+  else nl = in->auto_levels ? std::min(max_lv, in->max_levels) : std::min(8, max_lv);
+  if (nl < 1 || nl > 16) return -1;
+  o->num_levels = nl;
+  const double dxc = dx_fine * (double)(1L << (nl - 1));
+  o->dx_fine = dx_fine;
+  o->dx_coarse = dxc;
+  for (int l = 1; l <= nl; ++l) o->dx_levels[l - 1] = dx_fine * (double)(1L << (nl - l));
+  const int bs = in->block_size;
+  auto cells = [&](double d) {
+    const double c = std::ceil(std::ceil(d / dxc) / bs) * bs;
+    return std::max(bs, (int)c);
+  };
+  o->nx = cells(dx);
+  o->ny = cells(dy);
+  o->nz = cells(dz);
+  dx = o->nx * dxc;
+  dy = o->ny * dxc;
+  dz = o->nz * dxc;
+  o->domain[0] = dx;
+  o->domain[1] = dy;
+  o->domain[2] = dz;
+  o->bx = o->nx / bs;
+  o->by = o->ny / bs;
+  o->bz = o->nz / bs;
+  const double mesh_x = L * in->upstream;
+  const double mesh_y = in->symmetric ? 0.0 : (dy / 2 - ctr[1]);
+  const double mesh_z = dz / 2 - ctr[2];
+  o->offset[0] = mesh_x - mn[0];
+  o->offset[1] = mesh_y;
+  o->offset[2] = mesh_z;
+  o->length_scale = dx_fine;
+  o->velocity_scale = in->u_phys / (double)in->u_lattice;
+  o->time_scale = o->length_scale / o->velocity_scale;
+  o->nu_lattice = in->nu_phys * o->time_scale / (o->length_scale * o->length_scale);
+  // tau per level (:136-140): tau_l = 1/2 + (tau_f - 1/2) 2^(L-l), stored as Float32
+  for (int l = 1; l <= nl; ++l) {
+    const double t = l == nl ? tau_fine : 0.5 + (tau_fine - 0.5) * std::pow(2.0, nl - l);
+    o->tau_levels[l - 1] = (float)t;
+  }
+  // rho L^4 / T^2 (:142).  Julia evaluates x^2 as x*x and x^4 by compensated
+  // squaring (correctly rounded here), which libm's pow matches.
+  o->force_scale = in->rho_phys * std::pow(o->length_scale, 4.0) / (o->time_scale * o->time_scale);
+  o->moment_center[0] = mn[0] + o->offset[0] + in->moment_center[0] * o->ref_chord;
+  o->moment_center[1] = ctr[1] + o->offset[1] + in->moment_center[1] * o->ref_chord;
+  o->moment_center[2] = ctr[2] + o->offset[2] + in->moment_center[2] * o->ref_chord;
+  if (in->ddf_enabled) {
+    // thermal relaxation (:148-159): kappa = nu_lattice / Pr
+    const double kappa = o->nu_lattice / in->prandtl;
+    o->tau_g_fine = 0.5 + 3.0 * kappa;
+    for (int l = 1; l <= nl; ++l) {
+      const double t = l == nl ? o->tau_g_fine : 0.5 + (o->tau_g_fine - 0.5) * std::pow(2.0, nl - l);
+      o->tau_g_levels[l - 1] = (float)t;
+    }
+  }
+  return 0;
+}
+
 }  // extern "C"

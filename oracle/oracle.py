@@ -299,6 +299,72 @@ def merged_output(levels: list, t_step: int) -> dict:
     return out
 
 
+class ScaleInC(C.Structure):
+    _fields_ = [("mesh_min", C.c_double * 3), ("mesh_max", C.c_double * 3),
+                ("ref_length_cfg", C.c_double), ("ref_dim", C.c_int32),
+                ("ref_chord_cfg", C.c_double), ("ref_area_cfg", C.c_double),
+                ("symmetric", C.c_int32), ("moment_center", C.c_double * 3),
+                ("u_phys", C.c_double), ("nu_phys", C.c_double), ("rho_phys", C.c_double),
+                ("surface_resolution", C.c_int32), ("u_lattice", C.c_float),
+                ("tau_min", C.c_float), ("upstream", C.c_double), ("downstream", C.c_double),
+                ("lateral", C.c_double), ("height", C.c_double), ("block_size", C.c_int32),
+                ("min_coarse_blocks", C.c_int32), ("num_levels_cfg", C.c_int32),
+                ("auto_levels", C.c_int32), ("max_levels", C.c_int32),
+                ("ddf_enabled", C.c_int32), ("prandtl", C.c_double)]
+
+
+class ScaleOutC(C.Structure):
+    _fields_ = [("num_levels", C.c_int32), ("nx", C.c_int32), ("ny", C.c_int32),
+                ("nz", C.c_int32), ("bx", C.c_int32), ("by", C.c_int32), ("bz", C.c_int32),
+                ("ref_length", C.c_double), ("ref_chord", C.c_double), ("ref_area", C.c_double),
+                ("re", C.c_double), ("tau_fine", C.c_double), ("domain", C.c_double * 3),
+                ("offset", C.c_double * 3), ("moment_center", C.c_double * 3),
+                ("dx_fine", C.c_double), ("dx_coarse", C.c_double), ("dx_levels", C.c_double * 16),
+                ("length_scale", C.c_double), ("velocity_scale", C.c_double),
+                ("time_scale", C.c_double), ("nu_lattice", C.c_double),
+                ("force_scale", C.c_double), ("tau_levels", C.c_float * 16),
+                ("tau_g_fine", C.c_double), ("tau_g_levels", C.c_float * 16)]
+
+
+def domain_scaling(cfg, mesh_min, mesh_max) -> dict:
+    """compute_domain_from_mesh (physics_scaling.jl:83-191) from a CaseConfig
+    and the mesh bounds; returns the scaled quantities as a dict."""
+    s = ScaleInC()
+    s.mesh_min[:] = [float(v) for v in mesh_min]
+    s.mesh_max[:] = [float(v) for v in mesh_max]
+    s.ref_length_cfg = cfg.reference_length_for_meshing
+    s.ref_dim = {"x": 0, "y": 1, "z": 2}.get(cfg.reference_dimension, 3)
+    s.ref_chord_cfg, s.ref_area_cfg = cfg.reference_chord_config, cfg.reference_area_config
+    s.symmetric = int(bool(cfg.symmetric_analysis))
+    s.moment_center[:] = [float(v) for v in cfg.moment_center]
+    s.u_phys, s.nu_phys = cfg.flow_velocity, cfg.fluid_kinematic_viscosity
+    s.rho_phys = cfg.fluid_density
+    s.surface_resolution = cfg.surface_resolution
+    s.u_lattice, s.tau_min = cfg.u_target, cfg.tau_min
+    s.upstream, s.downstream = cfg.domain_upstream, cfg.domain_downstream
+    s.lateral, s.height = cfg.domain_lateral, cfg.domain_height
+    s.block_size, s.min_coarse_blocks = cfg.block_size, cfg.min_coarse_blocks
+    s.num_levels_cfg, s.auto_levels = cfg.num_levels_config, int(bool(cfg.auto_levels))
+    s.max_levels, s.ddf_enabled = cfg.max_levels, int(bool(cfg.ddf_enabled))
+    s.prandtl = cfg.ddf_prandtl
+    o = ScaleOutC()
+    fn = lib().orc_domain_scaling
+    fn.restype = C.c_int
+    if fn(C.byref(s), C.byref(o)) != 0:
+        raise ValueError("level count outside 1..16")
+    nl = o.num_levels
+    return dict(num_levels=nl, nx_coarse=o.nx, ny_coarse=o.ny, nz_coarse=o.nz, bx_max=o.bx,
+                by_max=o.by, bz_max=o.bz, reference_length=o.ref_length,
+                reference_chord=o.ref_chord, reference_area=o.ref_area, re_number=o.re,
+                tau_fine=o.tau_fine, domain_size=tuple(o.domain), mesh_offset=tuple(o.offset),
+                moment_center=tuple(o.moment_center), dx_fine=o.dx_fine, dx_coarse=o.dx_coarse,
+                dx_levels=list(o.dx_levels[:nl]), length_scale=o.length_scale,
+                velocity_scale=o.velocity_scale, time_scale=o.time_scale,
+                nu_lattice=o.nu_lattice, force_scale=o.force_scale,
+                tau_levels=[float(v) for v in o.tau_levels[:nl]], tau_g_fine=o.tau_g_fine,
+                tau_g_levels=[float(v) for v in o.tau_g_levels[:nl]] if cfg.ddf_enabled else [])
+
+
 def double_to_half_bits(x: float) -> int:
     fn = lib().orc_double_to_half
     fn.restype = C.c_uint16

@@ -106,6 +106,21 @@ def test_simulation_writes_merged_output(tmp_path):
     sim = S.Simulation(c, mesh, p, hosts, torch.device("cuda:0"))
     sim.run(8, diag_freq=8, output_dir=str(tmp_path))
     names = sorted(f.name for f in tmp_path.iterdir())
-    assert names == ["flow_000004.vtu", "flow_000008.vtu"]
+    assert names == ["convergence.csv", "flow_000004.vtu", "flow_000008.vtu", "forces.csv",
+                     "surface_000004.lbmp", "surface_000008.lbmp"]
     raw = (tmp_path / "flow_000008.vtu").read_bytes()
     assert f'NumberOfCells="{512 * hosts[0].n_blocks}"'.encode() in raw
+    # output step 4 is not a diagnostics multiple: its force sample is
+    # accumulated too (main.jl:267-275); step 8 is the diagnostics sample
+    assert sim.n_avg == 2 and len(sim.history) == 1
+    from openludwig_b200 import records as R
+    conv = (tmp_path / "convergence.csv").read_text().splitlines()
+    forces = (tmp_path / "forces.csv").read_text().splitlines()
+    assert conv[0] == R.CONVERGENCE_HEADER and len(conv) == 2 and conv[1].startswith("8,")
+    assert forces[0] == R.FORCE_HEADER and len(forces) == 2
+    fr, _, maps = sim.forces(maps=True)
+    assert forces[1] == R.force_row(8, 8 * p.time_scale, fr, sim.history[0]["u"])
+    got = R.read_surface_pressure_bin(str(tmp_path / "surface_000008.lbmp"))
+    m = maps.cpu().numpy()
+    assert got["pressure"].shape == (mesh.n,) and np.array_equal(got["pressure"], m[0])
+    assert np.array_equal(got["shear"], np.sqrt(m[1] * m[1] + m[2] * m[2] + m[3] * m[3]))
