@@ -78,7 +78,9 @@ def _level_dict(lv: OLevel, f_out, f_in, vel_out, vel_in, store_post):
 
 
 def perform_timestep(s: dict, lv: OLevel, parent, f_out, f_in, vel_out, vel_in, g_out, g_in,
-                     u: float, t_sub: int, tw: float, domain_dims, dtype):
+                     u: float, t_sub: int, tw: float, domain_dims, dtype, k=orc):
+    """timestep.jl:1-159 on one level; `k` is the kernel set (the CPU oracle,
+    or oracle.gpu over device tensors)."""
     h = lv.host
     is_l1 = parent is None
     scale = 1 << (h.level_id - 1)
@@ -94,10 +96,10 @@ def perform_timestep(s: dict, lv: OLevel, parent, f_out, f_in, vel_out, vel_in, 
         pv = dict(f=parent["f"], rho=parent["rho"], vel=parent["vel"], f_old=parent["f_old"],
                   rho_old=parent["rho_old"], vel_old=parent["vel_old"],
                   block_ptr=parent["block_ptr"], dim=parent["dim"], n_blocks=parent["n_blocks"])
-    orc.stream_collide(_level_dict(lv, f_out, f_in, vel_out, vel_in, bz), pv, params, dtype)
+    k.stream_collide(_level_dict(lv, f_out, f_in, vel_out, vel_in, bz), pv, params, dtype)
     if bz:
-        orc.bouzidi(f_out, lv.f_post, h.q_map, h.cell_block, h.cell_x, h.cell_y, h.cell_z,
-                    h.neighbor_table, h.n_blocks, s["q_min"], dtype)
+        k.bouzidi(f_out, lv.f_post, h.q_map, h.cell_block, h.cell_x, h.cell_y, h.cell_z,
+                  h.neighbor_table, h.n_blocks, s["q_min"], dtype)
     if s.get("ddf") and g_out is not None:
         tp = dict(tau_g=h.tau_g, tau_g_parent=parent["tau_g"] if parent else 0.5,
                   is_level_1=int(is_l1), is_symmetric=s["is_symmetric"], nx_global=dims[0],
@@ -114,13 +116,15 @@ def perform_timestep(s: dict, lv: OLevel, parent, f_out, f_in, vel_out, vel_in, 
             tpv = dict(g=parent["g"], T=parent["T"], vel=parent["vel"], g_old=parent["g_old"],
                        T_old=parent["T_old"], vel_old=parent["vel_old"],
                        block_ptr=parent["block_ptr"], dim=parent["dim"], n_blocks=parent["n_blocks"])
-        orc.thermal(tv, tpv, tp, dtype)
+        k.thermal(tv, tpv, tp, dtype)
         if bz:
-            orc.bouzidi(g_out, lv.g_post, h.q_map, h.cell_block, h.cell_x, h.cell_y, h.cell_z,
-                        h.neighbor_table, h.n_blocks, s["q_min"], dtype)
+            k.bouzidi(g_out, lv.g_post, h.q_map, h.cell_block, h.cell_x, h.cell_y, h.cell_z,
+                      h.neighbor_table, h.n_blocks, s["q_min"], dtype)
 
 
-def recursive_step(levels, s, lvl, t_sub, parent, tw, u, domain_dims, dtype):
+def recursive_step(levels, s, lvl, t_sub, parent, tw, u, domain_dims, dtype, k=orc):
+    """solver_control.jl:6-98 (copy_to_old! before a parent step, children
+    at (2t, tw 0) and (2t+1, tw 1/2))."""
     if lvl >= len(levels):
         return
     lv = levels[lvl]
@@ -132,24 +136,24 @@ def recursive_step(levels, s, lvl, t_sub, parent, tw, u, domain_dims, dtype):
         g_in, g_out = lv.g_temp, lv.g
     has_children = lvl + 1 < len(levels)
     if has_children and s["use_temporal_interp"]:
-        np.copyto(lv.f_old, f_in)
-        np.copyto(lv.rho_old, lv.rho)
-        np.copyto(lv.vel_old, vel_in)
+        k.copyto(lv.f_old, f_in)
+        k.copyto(lv.rho_old, lv.rho)
+        k.copyto(lv.vel_old, vel_in)
         if s.get("ddf") and lv.g is not None:
-            np.copyto(lv.g_old, g_in)
-            np.copyto(lv.T_old, lv.T)
+            k.copyto(lv.g_old, g_in)
+            k.copyto(lv.T_old, lv.T)
     perform_timestep(s, lv, parent, f_out, f_in, vel_out, vel_in, g_out, g_in, u, t_sub,
-                     0.0 if parent is None else tw, domain_dims, dtype)
+                     0.0 if parent is None else tw, domain_dims, dtype, k)
     if has_children:
         h = lv.host
         me = dict(f=f_out, rho=lv.rho, vel=vel_out, f_old=lv.f_old, rho_old=lv.rho_old,
                   vel_old=lv.vel_old, block_ptr=h.block_ptr, dim=h.grid_dim, n_blocks=h.n_blocks,
                   tau=h.tau, tau_g=h.tau_g, g=g_out, T=lv.T, g_old=lv.g_old, T_old=lv.T_old)
-        recursive_step(levels, s, lvl + 1, 2 * t_sub, me, 0.0, u, domain_dims, dtype)
-        recursive_step(levels, s, lvl + 1, 2 * t_sub + 1, me, 0.5, u, domain_dims, dtype)
+        recursive_step(levels, s, lvl + 1, 2 * t_sub, me, 0.0, u, domain_dims, dtype, k)
+        recursive_step(levels, s, lvl + 1, 2 * t_sub + 1, me, 0.5, u, domain_dims, dtype, k)
         if s.get("restriction"):
             c = levels[lvl + 1]   # its second sub-step (odd t_sub) wrote f and vel
-            orc.restrict(c.f, c.host.obstacle, c.host.map_x, c.host.map_y, c.host.map_z,
+            k.restrict(c.f, c.host.obstacle, c.host.map_x, c.host.map_y, c.host.map_z,
                          c.host.n_blocks, f_out, lv.rho, vel_out, h.obstacle, h.block_ptr,
                          h.grid_dim, h.n_blocks, c.host.tau, h.tau, s["compressible_corr"], dtype)
 

@@ -25,7 +25,8 @@ _lib = None
 
 def build(force: bool = False) -> Path:
     """Compile the oracle with its Makefile (g++, -ffp-contract=off, OpenMP)."""
-    srcs = [HERE / "ol_oracle_kernels.cpp", HERE / "ol_oracle_domain.cpp", HERE / "Makefile"]
+    srcs = [HERE / "ol_oracle_kernels.cpp", HERE / "ol_oracle_domain.cpp",
+            HERE / "ol_oracle_cell.h", HERE / "Makefile"]
     if force or not LIB_PATH.exists() or any(s.stat().st_mtime > LIB_PATH.stat().st_mtime for s in srcs):
         r = subprocess.run(["make", "-C", str(HERE), "-B" if force else "all"],
                            capture_output=True, text=True)
@@ -45,6 +46,9 @@ def lib() -> C.CDLL:
 
 def _p(a):
     return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+copyto = np.copyto
 
 
 class StepParamsC(C.Structure):
