@@ -606,6 +606,43 @@ OL_API int ol_bouzidi_qmap(const int32_t *coords, int32_t n_blocks, const double
                            double dx, const double offset[3], uint16_t *q_map,
                            int32_t *tri_map, uint8_t *has_link, void *stream);
 
+/* ------------------------------------------------------------------------
+ * FE load mapping: net triangle forces to structural nodes
+ * (PREPOST/map_forces_to_nodes.jl).  Each triangle force, applied at its
+ * centroid c, goes to the k = min(3, nodes of its object) nearest nodes of
+ * the same object (squared distances in FP64, ties to the earlier node) as
+ * the minimum-norm solution of
+ *   sum_i F_i = F,   sum_i (p_i - c) x F_i = 0,   f = pinv(A) b
+ * (A 6 x 3k, singular values at or below 6 eps sigma_max dropped, as
+ * LinearAlgebra.pinv does; map_forces_to_nodes.jl:143-231); the nodal load is
+ * the sum over triangles.  Nodes and triangles are grouped by object: object
+ * o owns nodes [node_begin[o], node_begin[o+1]) and triangles [tri_begin[o],
+ * tri_begin[o+1]); an object without nodes leaves its triangles unassigned
+ * (node -1, force 0), as the reference skips it.  The sums are exact in
+ * per-node fixed point (2^-40 of the node's largest contribution), so the
+ * result does not depend on the order the GPU adds in.
+ * All arrays are device memory; xyz triples are stored as three planes.
+ * ------------------------------------------------------------------------ */
+typedef struct ol_fe_map_view {
+  const double *node_xyz;       /* [3 * n_nodes]                                   */
+  const double *tri_xyz;        /* [3 * n_tris] centroids                         */
+  const double *tri_force;      /* [3 * n_tris]                                   */
+  const int32_t *node_begin;    /* [n_objects + 1], node_begin[0] = 0             */
+  const int32_t *tri_begin;     /* [n_objects + 1], tri_begin[0] = 0              */
+  int32_t n_nodes, n_tris, n_objects;
+  int32_t *tri_nodes;           /* out [3 * n_tris]: node of slot j (nearest first) at j * n_tris + t, -1 unused */
+  double *tri_node_force;       /* out [9 * n_tris]: component c of slot j at (3 j + c) * n_tris + t */
+  double *nodal_force;          /* out [3 * n_nodes]                               */
+  void *scratch;                /* ol_fe_map_scratch_bytes(n_nodes) bytes           */
+} ol_fe_map_view;
+/* Bytes of device scratch ol_fe_map_forces needs for n_nodes nodes. */
+OL_API size_t ol_fe_map_scratch_bytes(int32_t n_nodes);
+/* Map the forces on `stream` and wait for it.  *n_unconverged (host) = the
+ * triangles whose SVD sweep limit was reached (their result is still the
+ * last iterate).  OL_ERR_ARG for inconsistent sizes or more than 2^21
+ * contributions to one node. */
+OL_API int ol_fe_map_forces(const ol_fe_map_view *v, int32_t *n_unconverged, void *stream);
+
 /* Message of the last failing call on this thread. */
 OL_API const char *ol_last_error(void);
 /* Library version string. */

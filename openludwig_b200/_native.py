@@ -81,6 +81,12 @@ class RestrictView(C.Structure):
                 ("tau_coarse", f32), ("compressible", i32)]
 
 
+class FeMapView(C.Structure):
+    _fields_ = [("node_xyz", vp), ("tri_xyz", vp), ("tri_force", vp), ("node_begin", vp),
+                ("tri_begin", vp), ("n_nodes", i32), ("n_tris", i32), ("n_objects", i32),
+                ("tri_nodes", vp), ("tri_node_force", vp), ("nodal_force", vp), ("scratch", vp)]
+
+
 class SurfaceMesh(C.Structure):
     _fields_ = [("cx", vp), ("cy", vp), ("cz", vp), ("nx", vp), ("ny", vp), ("nz", vp),
                 ("area", vp), ("n_triangles", i32)]
@@ -220,6 +226,8 @@ _SIGS = {
     "ol_serve_history": (C.c_int, [vp, i32, C.POINTER(C.c_double), i32, C.POINTER(i32)]),
     "ol_ctx_stats": (C.c_int, [vp, C.POINTER(C.c_size_t), C.POINTER(C.c_size_t),
                                C.POINTER(i32), C.POINTER(C.c_int64)]),
+    "ol_fe_map_scratch_bytes": (C.c_size_t, [i32]),
+    "ol_fe_map_forces": (C.c_int, [C.POINTER(FeMapView), C.POINTER(i32), vp]),
     "ol_last_error": (C.c_char_p, []),
     "ol_version": (C.c_char_p, []),
 }

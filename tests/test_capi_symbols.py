@@ -68,6 +68,7 @@ def test_argument_errors_are_reported_not_raised(lib):
     assert lib.ol_ctx_case_step(None, 0, 1, ctypes.c_float(-1.0)) == 1
     assert lib.ol_ctx_case_coefficients(None, 0, None, None) == 1
     assert lib.ol_set_stream_collide_kernel(7, 0) == 1
+    assert lib.ol_fe_map_forces(None, None, None) == 1
 
 
 def test_ctypes_struct_layouts_match_header(tmp_path):
@@ -87,7 +88,7 @@ def test_ctypes_struct_layouts_match_header(tmp_path):
              "ol_net_force_maps": N.NetForceMaps, "ol_output_level": N.OutputLevel,
              "ol_output_fields": N.OutputFields, "ol_bouzidi_link": N.BouzidiLink,
              "ol_coeff_ref": N.CoeffRef, "ol_serve_rule": N.ServeRule,
-             "ol_serve_result": N.ServeResult}
+             "ol_serve_result": N.ServeResult, "ol_fe_map_view": N.FeMapView}
     src = tmp_path / "sizes.c"
     src.write_text('#include <stdio.h>\n#include "openludwig_b200.h"\nint main(void){\n' +
                    "".join(f'printf("%zu\\n", sizeof({n}));\n' for n in names) + "return 0;}\n")
