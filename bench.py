@@ -345,6 +345,49 @@ def bench_served(a, dev, local, batched) -> dict:
     return out
 
 
+def kernel_times(a, local) -> None:
+    """Per-kernel device time of the drop-in coarse step of the workload:
+    a.warmup eager steps, then a.steps steps under the torch profiler
+    (CUPTI activity records; caches warm, launches as the C-ABI path issues
+    them).  One JSON line: microseconds per coarse step and share, per kernel."""
+    import collections
+
+    import torch
+    from torch.profiler import ProfilerActivity, profile
+
+    from openludwig_b200 import build as olbuild
+    olbuild.build()
+    from openludwig_b200 import solver as S
+    cfg, mesh, p, hosts = build_case(a.workload)
+    dev = torch.device("cuda", local)
+    levels = [S.upload_level(h, dev, ddf=bool(cfg.ddf_enabled)) for h in hosts]
+    st = S.StepSettings.from_config(cfg, cfg.wall_model_enabled)
+    dims = (p.nx_coarse, p.ny_coarse, p.nz_coarse)
+    u = float(cfg.u_target)
+    t = 0
+    for _ in range(a.warmup):
+        t += 1
+        S.recursive_step(levels, st, 0, t, None, 0.0, u, dims)
+    torch.cuda.synchronize()
+    n = max(1, a.steps)
+    with profile(activities=[ProfilerActivity.CUDA]) as prof:
+        for _ in range(n):
+            t += 1
+            S.recursive_step(levels, st, 0, t, None, 0.0, u, dims)
+        torch.cuda.synchronize()
+    agg = collections.defaultdict(lambda: [0, 0.0])
+    for ev in prof.events():
+        if ev.device_type == torch.autograd.DeviceType.CUDA:
+            agg[ev.name][0] += 1
+            agg[ev.name][1] += ev.device_time_total
+    total = sum(v[1] for v in agg.values())
+    rows = [{"kernel": k, "launches_per_step": c / n, "us_per_step": us / n,
+             "share": us / total if total else 0.0}
+            for k, (c, us) in sorted(agg.items(), key=lambda kv: -kv[1][1])]
+    print(json.dumps({"workload": a.workload, "coarse_steps": n, "warmup": a.warmup,
+                      "us_per_step_total": total / n, "kernels": rows}), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -360,6 +403,9 @@ def main():
     ap.add_argument("--served-requests", type=int, default=24,
                     help="requests of the served sample (config 5 asks for 500)")
     ap.add_argument("--launcher-selftest", action="store_true", help=argparse.SUPPRESS)
+    ap.add_argument("--kernel-times", action="store_true",
+                    help="print the device time of each kernel per coarse step of the drop-in "
+                         "path (torch profiler, warm, eager launches) instead of the bench line")
     a = ap.parse_args()
     a.warmup = max(a.warmup, 3)
 
@@ -416,6 +462,10 @@ def main():
     if not torch.cuda.is_available():
         raise SystemExit("bench.py needs a CUDA device")
     torch.cuda.set_device(local)
+    if a.kernel_times:
+        if rank == 0:
+            kernel_times(a, local)
+        return
     if world > 1:
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
     from openludwig_b200 import replicas
