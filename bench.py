@@ -345,6 +345,39 @@ def bench_served(a, dev, local, batched) -> dict:
     return out
 
 
+def pool_probe(a, local) -> None:
+    """The block pool's coarse step of the workload alone, with a chosen
+    storage and stream-collide kernel (ol_set_stream_collide_kernel): a.warmup
+    steps, then a.steps timed by Context.step_timed (CUDA events)."""
+    import torch
+
+    from openludwig_b200 import _native as N
+    from openludwig_b200 import build as olbuild
+    olbuild.build()
+    from openludwig_b200 import native as NT
+    from openludwig_b200 import solver as S
+    storage, kernel = a.pool_probe.split(":")
+    choice = {"auto": 0, "block": 1, "ws": 2}[kernel]
+    torch.cuda.set_device(local)
+    cfg, mesh, p, hosts = build_case(a.workload)
+    case = NT.PreparedCase(cfg, mesh, p, hosts, S.StepSettings.from_config(cfg, cfg.wall_model_enabled))
+    upd = sum(h.n_blocks * 512 * (1 << i) for i, h in enumerate(hosts))
+    N.call("ol_set_stream_collide_kernel", N.i32(choice), N.i32(0))
+    try:
+        ctx = NT.Context(device=local, budget_bytes=16 << 30, storage=storage)
+        ctx.add_case(case)
+        ctx.step(a.warmup)
+        ctx.sync()
+        k = max(1, a.steps)
+        ms = ctx.step_timed(k)
+        ctx.close()
+    finally:
+        N.call("ol_set_stream_collide_kernel", N.i32(0), N.i32(0))
+    print(json.dumps({"workload": a.workload, "storage": storage, "kernel": kernel,
+                      "coarse_steps": k, "MLUPS": upd * k / (ms / 1e3) / 1e6,
+                      "ms_per_step": ms / k}), flush=True)
+
+
 def kernel_times(a, local) -> None:
     """Per-kernel device time of the drop-in coarse step of the workload:
     a.warmup eager steps, then a.steps steps under the torch profiler
@@ -403,6 +436,10 @@ def main():
     ap.add_argument("--served-requests", type=int, default=24,
                     help="requests of the served sample (config 5 asks for 500)")
     ap.add_argument("--launcher-selftest", action="store_true", help=argparse.SUPPRESS)
+    ap.add_argument("--pool-probe", default=None, metavar="STORAGE:KERNEL",
+                    help="time only the block pool's coarse step of the workload with storage "
+                         "f32|f16 and stream-collide kernel auto|block|ws (e.g. f16:ws), one JSON "
+                         "line")
     ap.add_argument("--kernel-times", action="store_true",
                     help="print the device time of each kernel per coarse step of the drop-in "
                          "path (torch profiler, warm, eager launches) instead of the bench line")
@@ -465,6 +502,10 @@ def main():
     if a.kernel_times:
         if rank == 0:
             kernel_times(a, local)
+        return
+    if a.pool_probe:
+        if rank == 0:
+            pool_probe(a, local)
         return
     if world > 1:
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
