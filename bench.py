@@ -304,7 +304,49 @@ def bench_batched(a, dev, local, peak_gbs, plain_value) -> dict:
         ctx.close()
     out["f16_over_f32_batched"] = out["f16"]["MLUPS"] / out["f32"]["MLUPS"]
     out["f16_over_f32_plain"] = out["f16"]["MLUPS"] / plain_value
+    # the plain form on the same mix: each case alone through the FP32 drop-in
+    # path (ol_stream_collide / Bouzidi calls per level sub-step, as the
+    # reference's driver issues them), one case after another
+    serial = serial_plain_mix(a, dev, cases)
+    out["serial_f32_dropin_same_mix"] = serial
+    out["f16_over_f32_serial_same_mix"] = out["f16"]["MLUPS"] / serial["MLUPS"]
+    out["f32_over_f32_serial_same_mix"] = out["f32"]["MLUPS"] / serial["MLUPS"]
     return out
+
+
+def serial_plain_mix(a, dev, cases) -> dict:
+    """The cases one at a time on the plain FP32 drop-in path: per case its
+    levels are uploaded, a.warmup coarse steps run, then max(4, a.steps)
+    coarse steps are timed with CUDA events; MLUPS = all cases' cell updates
+    over the sum of their times."""
+    import torch
+
+    from openludwig_b200 import solver as S
+    k = max(4, a.steps)
+    upd_total, ms_total = 0, 0.0
+    stream = torch.cuda.Stream(device=dev)
+    for c in cases:
+        levels = [S.upload_level(h, dev, ddf=bool(c.cfg.ddf_enabled)) for h in c.levels]
+        dims = (c.params.nx_coarse, c.params.ny_coarse, c.params.nz_coarse)
+        u = float(c.cfg.u_target)
+        with torch.cuda.stream(stream):
+            t = 0
+            for _ in range(a.warmup):
+                t += 1
+                S.recursive_step(levels, c.settings, 0, t, None, 0.0, u, dims)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(k):
+                t += 1
+                S.recursive_step(levels, c.settings, 0, t, None, 0.0, u, dims)
+            e1.record(stream)
+        torch.cuda.synchronize()
+        ms_total += e0.elapsed_time(e1)
+        upd_total += c.cell_updates_per_step * k
+        del levels
+    return {"MLUPS": upd_total / (ms_total / 1e3) / 1e6, "ms_total": ms_total, "coarse_steps": k,
+            "cases": len(cases), "form": "FP32 drop-in path, one case at a time, eager C-ABI "
+            "calls per level sub-step, CUDA events per case"}
 
 
 def bench_served(a, dev, local, batched) -> dict:
@@ -341,7 +383,10 @@ def bench_served(a, dev, local, batched) -> dict:
     out["solves_per_hour"] = opened["solves_per_hour"]
     out["p50_s"], out["p99_s"] = opened["p50_s"], opened["p99_s"]
     out["served_over_serial"] = opened["solves_per_hour"] / serial["solves_per_hour"]
-    out["cd_err_vs_fp64"] = batched.get("cd_err_vs_fp64")
+    # capacities: closed-loop served rate against the serial form's rate when
+    # it is never idle (its requests over the sum of its solve times)
+    out["serial_capacity_solves_per_hour"] = n / serial["busy_s"] * 3600.0
+    out["capacity_over_serial"] = closed["solves_per_hour"] / out["serial_capacity_solves_per_hour"]
     return out
 
 

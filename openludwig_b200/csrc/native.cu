@@ -531,7 +531,7 @@ static void launch_variant(ol_ctx *c, const Launch &l) {
     if (choice == OL_SC_KERNEL_WS ||
         (f32 && c->grid_mult == kGridWs && choice == OL_SC_KERNEL_AUTO)) {
       const int grid = ws_grid(l.n, c->n_sm);
-      k_sc_ws<OP, ST, WALE, true><<<(unsigned)grid, kWsThreads, kWsBytes, c->stream>>>(
+      k_sc_ws<OP, ST, WALE, true><<<(unsigned)grid, kWsThreads, ws_smem_bytes<ST>(), c->stream>>>(
           LevelDev{}, c->d_descs, c->d_items + l.off, (int)l.n, ws_table_device(),
           fault_word_device());
       return;
@@ -835,10 +835,14 @@ static int prepare_attributes() {
   cudaFuncSetAttribute(k_sc_pipe<1, true, true>, (cudaFuncAttribute)a, kPipeBytes);
   prepare_attributes_st<StoreF32>();
   prepare_attributes_st<StoreF16S>();
-  cudaFuncSetAttribute(k_sc_ws<0, StoreF32, false, true>, (cudaFuncAttribute)a, kWsBytes);
-  cudaFuncSetAttribute(k_sc_ws<0, StoreF32, true, true>, (cudaFuncAttribute)a, kWsBytes);
-  cudaFuncSetAttribute(k_sc_ws<0, StoreF16S, false, true>, (cudaFuncAttribute)a, kWsBytes);
-  cudaFuncSetAttribute(k_sc_ws<0, StoreF16S, true, true>, (cudaFuncAttribute)a, kWsBytes);
+  cudaFuncSetAttribute(k_sc_ws<0, StoreF32, false, true>, (cudaFuncAttribute)a,
+                       ws_smem_bytes<StoreF32>());
+  cudaFuncSetAttribute(k_sc_ws<0, StoreF32, true, true>, (cudaFuncAttribute)a,
+                       ws_smem_bytes<StoreF32>());
+  cudaFuncSetAttribute(k_sc_ws<0, StoreF16S, false, true>, (cudaFuncAttribute)a,
+                       ws_smem_bytes<StoreF16S>());
+  cudaFuncSetAttribute(k_sc_ws<0, StoreF16S, true, true>, (cudaFuncAttribute)a,
+                       ws_smem_bytes<StoreF16S>());
   if (!fault_word_device() || !ws_table_device())
     return set_error(OL_ERR_CUDA, "warp-specialised kernel tables: allocation failed");
   const cudaError_t e = cudaGetLastError();

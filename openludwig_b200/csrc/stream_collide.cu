@@ -203,11 +203,11 @@ static void launch_ws(const LevelDev &L, int n_sm, cudaStream_t s) {
   static bool done = false;
   if (!done) {
     cudaFuncSetAttribute(k_sc_ws<OP, ST, WALE, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         kWsBytes);
+                         ws_smem_bytes<ST>());
     done = true;
   }
   const int grid = ws_grid(L.n_blocks, n_sm);
-  launch_pdl(k_sc_ws<OP, ST, WALE, false>, grid, kWsThreads, kWsBytes, s, L,
+  launch_pdl(k_sc_ws<OP, ST, WALE, false>, grid, kWsThreads, ws_smem_bytes<ST>(), s, L,
              (const LevelDev *)nullptr, (const WorkItem *)nullptr, 0, ws_table_device(),
              fault_word_device());
 }

@@ -9,18 +9,20 @@
 //     completion counted in bytes on an mbarrier) of item j+1's contiguous
 //     arrays: 27 population planes, 3 velocity planes, sponge, obstacle, wall
 //     distance -- 66 KB in FP32, moved without registers or request slots.
-//   * 16 consumer warps, one cell per thread, per item: spread the landed
-//     block into the compute stage -- populations "pre-streamed" (the value
-//     cell d pulls in direction k at F[k][d], so every pull is then one
-//     conflict-free shared load at a compile-time offset), FP16 decoded to
-//     FP32, velocities into 10^3 slots per component with a one-cell face
-//     halo (a face without neighbour repeats the cell beside it, the
-//     zero-gradient fallback of the WALE gradients) -- together with the
-//     out-of-block pull sources each thread loaded for this item one item
-//     earlier (a neighbour's value, the precomputed ghost value, or, without
-//     a ghost row, pull_boundary as in the one-CTA-per-block kernel); then
-//     release the landing buffer, issue the out-of-block loads of item j+1
-//     into registers, pull, collide and store straight to global memory.
+//   * 16 consumer warps, one cell per thread, per item: complete the compute
+//     stage -- with FP32 storage the population planes landed in it already,
+//     each shifted so that every pull is one conflict-free shared load at a
+//     compile-time offset (WsLayout); with FP16 storage they decode the
+//     landed block into a "pre-streamed" stage (the value cell d pulls in
+//     direction k at F[k][d]) -- by writing the out-of-block pull sources
+//     each thread loaded for this item one item earlier (a neighbour's value,
+//     the precomputed ghost value, or, without a ghost row, pull_boundary as
+//     in the one-CTA-per-block kernel) into the slots of the cells that pull
+//     them, and the velocities into 10^3 slots per component with a one-cell
+//     face halo (a face without neighbour repeats the cell beside it, the
+//     zero-gradient fallback of the WALE gradients); then pull, release the
+//     buffer the next bulk copies land in, issue the out-of-block loads of
+//     item j+1 into registers, collide and store straight to global memory.
 //     The next item's bulk copies and out-of-block loads land while they
 //     collide.
 // Why this split (measured on B200): a block is 66 KB, and an SM has to keep
@@ -53,19 +55,56 @@ constexpr int kWsRing = 4;  // descriptor / neighbour-offset slots (item j uses 
 // (face dir | own cell beside the slot << 5).
 constexpr int kWsVelEntries = 6 * 64;
 constexpr int kWsTableSize = kHaloEntries + kWsVelEntries;
-// landing buffer (bytes; the population planes are FP32 or FP16)
-constexpr int kLdF = 0;                                  // T [27][512]
-constexpr int kLdV = kLdF + 27 * BCELLS * 4;             // float [3][512]
-constexpr int kLdSP = kLdV + 3 * BCELLS * 4;             // float [512]
-constexpr int kLdWD = kLdSP + BCELLS * 4;                // float [512]
-constexpr int kLdOB = kLdWD + BCELLS * 4;                // uint8 [512]
-constexpr int kLdBytes = kLdOB + BCELLS;                 // 66,048
-// compute stage and table copy (bytes)
-constexpr int kWsF = kLdBytes;                           // float [27][512], pre-streamed
-constexpr int kWsV = kWsF + 27 * BCELLS * 4;             // float [3][1000]
-constexpr int kWsTab = kWsV + 3 * EPL * 4;               // uint32 [kWsTableSize]
-constexpr int kWsBytes = kWsTab + kWsTableSize * 4;      // 147,584 dynamic
-static_assert(kLdBytes % 16 == 0 && kWsV % 16 == 0, "alignment");
+// Dynamic shared memory (byte offsets).
+// FP32 storage ("direct"): the bulk copies land each population plane k
+// straight into the compute stage, shifted by 8 c_y + 64 c_z cells, so the
+// value cell t pulls in direction k sits at S[k][t - c_x]: no spread of the
+// landed block, one conflict-free shared load per pull.  A plane of the stage
+// holds 72 + 512 + 72 slots (the shifts reach 72 cells either way; every
+// landing address stays 32-byte aligned); the slots whose source lies
+// outside the block are then overwritten with the out-of-block values.  The
+// stage is the landing buffer, so it is free for the next item once the
+// consumers have pulled.  Velocity, sponge, wall distance and mask land
+// beside it.
+// FP16-shifted storage: the planes land in a buffer of their own and the
+// consumers decode them into a pre-streamed stage F[k][d] (the value cell d
+// pulls in direction k), releasing the buffer before they pull.
+constexpr int kSPad = 72;                         // stage slots before cell 0 (and after 511)
+constexpr int kSPlane = kSPad + BCELLS + kSPad;   // 656 floats = 2624 bytes
+template <class ST> struct WsLayout;
+template <> struct WsLayout<StoreF32> {
+  static constexpr bool kDirect = true;
+  static constexpr int kS = 0;                                  // float [27][kSPlane]
+  static constexpr int kV = kS + 27 * kSPlane * 4;              // float [3][1000]
+  static constexpr int kLdV = kV + 3 * EPL * 4;                 // float [3][512]
+  static constexpr int kLdSP = kLdV + 3 * BCELLS * 4;           // float [512]
+  static constexpr int kLdWD = kLdSP + BCELLS * 4;              // float [512]
+  static constexpr int kLdOB = kLdWD + BCELLS * 4;              // uint8 [512]
+  static constexpr int kTab = kLdOB + BCELLS;                   // uint32 [kWsTableSize]
+  static constexpr int kBytes = kTab + kWsTableSize * 4;        // 107,840
+  static constexpr int kLdF = 0, kF = 0;                        // (unused)
+};
+template <> struct WsLayout<StoreF16S> {
+  static constexpr bool kDirect = false;
+  static constexpr int kLdF = 0;                                // half [27][512]
+  static constexpr int kLdV = kLdF + 27 * BCELLS * 4;           // float [3][512]
+  static constexpr int kLdSP = kLdV + 3 * BCELLS * 4;           // float [512]
+  static constexpr int kLdWD = kLdSP + BCELLS * 4;              // float [512]
+  static constexpr int kLdOB = kLdWD + BCELLS * 4;              // uint8 [512]
+  static constexpr int kF = kLdOB + BCELLS;                     // float [27][512], pre-streamed
+  static constexpr int kV = kF + 27 * BCELLS * 4;               // float [3][1000]
+  static constexpr int kTab = kV + 3 * EPL * 4;                 // uint32 [kWsTableSize]
+  static constexpr int kBytes = kTab + kWsTableSize * 4;        // 147,584
+  static constexpr int kS = 0;                                  // (unused)
+};
+static_assert(WsLayout<StoreF32>::kV % 16 == 0 && WsLayout<StoreF32>::kLdV % 16 == 0 &&
+                  WsLayout<StoreF32>::kLdOB % 16 == 0 && (kSPlane * 4) % 32 == 0 &&
+                  (kSPad * 4) % 32 == 0,
+              "bulk-copy destinations stay 16-byte aligned");
+static_assert(WsLayout<StoreF16S>::kF % 16 == 0 && WsLayout<StoreF16S>::kV % 16 == 0,
+              "alignment");
+template <class ST>
+constexpr int ws_smem_bytes() { return WsLayout<ST>::kBytes; }
 constexpr int kWsHaloPerConsumer = (kHaloEntries + BCELLS - 1) / BCELLS;  // 7
 // A wait that has not completed after this long (ns) is treated as lost.
 constexpr unsigned long long kWsWaitNs = 2000000000ull;
@@ -173,6 +212,7 @@ template <class ST, bool WALE>
 __device__ __forceinline__ void ws_produce(const LevelDev &L, int b, int lane, unsigned char *ld,
                                            uint64_t *bar) {
   using T = typename ST::T;
+  using Lay = WsLayout<ST>;
   constexpr uint32_t kPlane = BCELLS * sizeof(T);
   const int64_t own0 = (L.block_offset + b) * BCELLS;
   const bool wd = L.sp.wall_model_active == 1 && L.wall_dist;
@@ -183,17 +223,22 @@ __device__ __forceinline__ void ws_produce(const LevelDev &L, int b, int lane, u
   __syncwarp();
   for (int c = lane; c < 33; c += 32) {
     if (c < 27) {
-      bulk_copy(ld + kLdF + c * kPlane, fin + (size_t)c * L.dstride + own0, kPlane, bar);
+      // direct: plane c shifted by 8 c_y + 64 c_z slots (a multiple of 8)
+      unsigned char *dst =
+          Lay::kDirect
+              ? ld + Lay::kS + (c * kSPlane + kSPad + 8 * cy_of(c) + 64 * cz_of(c)) * 4
+              : ld + Lay::kLdF + c * kPlane;
+      bulk_copy(dst, fin + (size_t)c * L.dstride + own0, kPlane, bar);
     } else if (c < 30) {
       if (WALE)
-        bulk_copy(ld + kLdV + (c - 27) * BCELLS * 4, L.vel_in + (size_t)(c - 27) * L.dstride + own0,
-                  BCELLS * 4, bar);
+        bulk_copy(ld + Lay::kLdV + (c - 27) * BCELLS * 4,
+                  L.vel_in + (size_t)(c - 27) * L.dstride + own0, BCELLS * 4, bar);
     } else if (c == 30) {
-      bulk_copy(ld + kLdSP, L.sponge + own0, BCELLS * 4, bar);
+      bulk_copy(ld + Lay::kLdSP, L.sponge + own0, BCELLS * 4, bar);
     } else if (c == 31) {
-      bulk_copy(ld + kLdOB, L.obstacle + own0, BCELLS, bar);
+      bulk_copy(ld + Lay::kLdOB, L.obstacle + own0, BCELLS, bar);
     } else if (wd) {
-      bulk_copy(ld + kLdWD, L.wall_dist + own0, BCELLS * 4, bar);
+      bulk_copy(ld + Lay::kLdWD, L.wall_dist + own0, BCELLS * 4, bar);
     }
   }
 }
@@ -242,13 +287,14 @@ __device__ __forceinline__ bool pull_inside(const CellMask &m, int k) {
   return (cx == 0 || (cx > 0 ? m.xhi : m.xlo)) && (cy == 0 || (cy > 0 ? m.yhi : m.ylo)) &&
          (cz == 0 || (cz > 0 ? m.zhi : m.zlo));
 }
-__device__ __forceinline__ float land_value(const unsigned char *ld, int k, int c, float, StoreF32) {
-  return ((const float *)(ld + kLdF))[k * BCELLS + c];
-}
 __device__ __forceinline__ float land_value(const unsigned char *ld, int k, int c, float inv_scale,
                                             StoreF16S) {
   const float w = w_of(k);
-  return fmaf(__half2float(((const __half *)(ld + kLdF))[k * BCELLS + c]), w * inv_scale, w);
+  return fmaf(__half2float(((const __half *)(ld + WsLayout<StoreF16S>::kLdF))[k * BCELLS + c]),
+              w * inv_scale, w);
+}
+__device__ __forceinline__ float land_value(const unsigned char *, int, int, float, StoreF32) {
+  return 0.0f;  // (direct layout: no spread)
 }
 template <int OP, class ST, bool WALE, bool BATCHED>
 __global__ void __launch_bounds__(kWsThreads, 1)
@@ -262,7 +308,8 @@ __global__ void __launch_bounds__(kWsThreads, 1)
   __shared__ __align__(8) uint64_t bars[2];  // landed, free
   uint64_t *const landed = &bars[0], *const lfree = &bars[1];
   unsigned char *const ld = ws_smem;
-  uint32_t *const tabs = (uint32_t *)(ws_smem + kWsTab);
+  using Lay = WsLayout<ST>;
+  uint32_t *const tabs = (uint32_t *)(ws_smem + Lay::kTab);
   const int t = threadIdx.x;
   const int n = BATCHED ? n_items : L0.n_blocks;
   const int first = blockIdx.x;
@@ -321,8 +368,8 @@ __global__ void __launch_bounds__(kWsThreads, 1)
   }
 
   // -------------------------------------------------------------- consumers
-  float *const F = (float *)(ws_smem + kWsF);
-  float *const V = (float *)(ws_smem + kWsV);
+  float *const F = (float *)(ws_smem + (Lay::kDirect ? Lay::kS : Lay::kF));
+  float *const V = (float *)(ws_smem + Lay::kV);
   const int x = t & 7, y = (t >> 3) & 7, z = t >> 6;
   const CellMask cm{x > 0, x < 7, y > 0, y < 7, z > 0, z < 7};
   const int eo = e_index(x, y, z);
@@ -335,12 +382,15 @@ __global__ void __launch_bounds__(kWsThreads, 1)
     const int *nbase = nbb[r];
     const int b = blk[r];
     if (j == 0) ws_halo_load<ST, WALE>(L, b, nbase, t, tabs, h);
-    // spread the landed block and this thread's out-of-block values into the stage
+    if constexpr (!Lay::kDirect) {
+      // spread the landed block into the pre-streamed stage
 #pragma unroll
-    for (int k = 0; k < 27; ++k)
-      if (pull_inside(cm, k))
-        F[k * BCELLS + t + cx_of(k) + 8 * cy_of(k) + 64 * cz_of(k)] =
-            land_value(ld, k, t, L.inv_scale, ST{});
+      for (int k = 0; k < 27; ++k)
+        if (pull_inside(cm, k))
+          F[k * BCELLS + t + cx_of(k) + 8 * cy_of(k) + 64 * cz_of(k)] =
+              land_value(ld, k, t, L.inv_scale, ST{});
+    }
+    // this thread's out-of-block values into the slots of the cells that pull them
     const bool ghost = ghost_row_of(L, b) != nullptr;
 #pragma unroll
     for (int m = 0; m < kWsHaloPerConsumer; ++m) {
@@ -348,13 +398,14 @@ __global__ void __launch_bounds__(kWsThreads, 1)
       if (i >= kHaloEntries) continue;
       const uint32_t e = tabs[i];
       const int k = e & 31, dir = (e >> 5) & 31, d = e >> 19;
-      if (nbase[dir] >= 0 || ghost)
-        F[k * BCELLS + d] = h.f[m];
-      else
-        F[k * BCELLS + d] = pull_boundary<ST>(L, k, b, d & 7, (d >> 3) & 7, d >> 6);
+      const float v = (nbase[dir] >= 0 || ghost)
+                          ? h.f[m]
+                          : pull_boundary<ST>(L, k, b, d & 7, (d >> 3) & 7, d >> 6);
+      if constexpr (Lay::kDirect) F[k * kSPlane + kSPad + d - cx_of(k)] = v;
+      else F[k * BCELLS + d] = v;
     }
     if (WALE) {
-      const float *lv = (const float *)(ld + kLdV);
+      const float *lv = (const float *)(ld + Lay::kLdV);
 #pragma unroll
       for (int c = 0; c < 3; ++c) V[c * EPL + eo] = lv[c * BCELLS + t];
       if (t < kWsVelEntries) {
@@ -367,23 +418,37 @@ __global__ void __launch_bounds__(kWsThreads, 1)
       }
     }
     CellAux aux;
-    aux.wall_dist = ((const float *)(ld + kLdWD))[t];
-    const float spg = ((const float *)(ld + kLdSP))[t];
-    const bool obs = ld[kLdOB + t] != 0;
-    // the landing buffer is read: the producer may fill it with item j+1
-    if (j + 1 < cnt) {
-      __syncwarp();
-      if ((t & 31) == 0) mbar_arrive(lfree);
+    aux.wall_dist = ((const float *)(ld + Lay::kLdWD))[t];
+    const float spg = ((const float *)(ld + Lay::kLdSP))[t];
+    const bool obs = ld[Lay::kLdOB + t] != 0;
+    if constexpr (!Lay::kDirect) {
+      // the landing buffer is read: the producer may fill it with item j+1
+      if (j + 1 < cnt) {
+        __syncwarp();
+        if ((t & 31) == 0) mbar_arrive(lfree);
+      }
     }
     consumer_sync();  // the stage holds item j
+    float A[27];
+    if constexpr (Lay::kDirect) {
+#pragma unroll
+      for (int k = 0; k < 27; ++k) A[k] = F[k * kSPlane + kSPad + t - cx_of(k)];
+      // the stage (also the landing buffer) is read: order these shared-memory
+      // accesses before the bulk copies of item j+1, then release it
+      if (j + 1 < cnt) {
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncwarp();
+        if ((t & 31) == 0) mbar_arrive(lfree);
+      }
+    } else {
+#pragma unroll
+      for (int k = 0; k < 27; ++k) A[k] = F[k * BCELLS + t];
+    }
     // item j+1's out-of-block values, in flight while item j collides
     if (j + 1 < cnt) {
       const int r1 = (j + 1) & (kWsRing - 1);
       ws_halo_load<ST, WALE>(BATCHED ? Ls[r1] : L0, blk[r1], nbb[r1], t, tabs, h);
     }
-    float A[27];
-#pragma unroll
-    for (int k = 0; k < 27; ++k) A[k] = F[k * BCELLS + t];
     if (WALE) {
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
