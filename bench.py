@@ -369,6 +369,11 @@ def bench_served(a, dev, local, batched) -> dict:
     ctx = NT.Context(device=local, budget_bytes=budget, storage="f16")
     closed = SV.Server(ctx, **rule).run([SV.Request(i, 0.0, mk) for i, mk in enumerate(makers)])
     ctx.close()
+    # the same closed loop with FP32 storage in the pool (the service's form
+    # when storage precision is not traded for bytes)
+    ctx = NT.Context(device=local, budget_bytes=budget, storage="f32")
+    closed32 = SV.Server(ctx, **rule).run([SV.Request(i, 0.0, mk) for i, mk in enumerate(makers)])
+    ctx.close()
     rate = 0.8 * closed["solves_per_hour"] / 3600.0
     arrivals = SV.poisson_arrivals(n, rate, seed=4321)
     ctx = NT.Context(device=local, budget_bytes=budget, storage="f16")
@@ -387,6 +392,9 @@ def bench_served(a, dev, local, batched) -> dict:
     # it is never idle (its requests over the sum of its solve times)
     out["serial_capacity_solves_per_hour"] = n / serial["busy_s"] * 3600.0
     out["capacity_over_serial"] = closed["solves_per_hour"] / out["serial_capacity_solves_per_hour"]
+    out["capacity_closed_loop_f32_storage"] = summary(closed32)
+    out["capacity_f32_storage_over_serial"] = (closed32["solves_per_hour"] /
+                                               out["serial_capacity_solves_per_hour"])
     return out
 
 
