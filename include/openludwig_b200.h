@@ -498,11 +498,21 @@ OL_API int ol_ctx_case_info(ol_ctx *ctx, int32_t case_id, int64_t *coarse_steps,
 #define OL_LAUNCH_WS (-2)
 #define OL_LAUNCH_PIPELINED (-1)
 #define OL_LAUNCH_PER_ITEM 0
+/* set_launch applies one shape to every collision variant (and clears the
+ * per-variant shapes the autotuner may have set). */
 OL_API int ol_ctx_set_launch(ol_ctx *ctx, int32_t shape);
 OL_API int ol_ctx_get_launch(ol_ctx *ctx, int32_t *shape);
-/* Times one coarse step of the resident mix (CUDA events) under each launch
- * shape above and keeps the fastest.  The timing replays advance every
- * resident case by 5 * (trials + 1) coarse steps. */
+/* Shape of the stream-collide launches of one collision variant (operator,
+ * WALE on/off, DDF on/off): the autotuner's choice for it, else the
+ * context's shape. */
+OL_API int ol_ctx_get_variant_launch(ol_ctx *ctx, int32_t op, int32_t wale, int32_t ddf,
+                                     int32_t *shape);
+/* Times `trials` coarse steps of the resident mix (CUDA events) under each
+ * launch shape above and keeps the fastest for the whole mix; then, when the
+ * mix holds more than one collision variant, tries each shape for one variant
+ * at a time (the others held) and keeps each variant's fastest.  The timing
+ * runs advance every resident case by 5 * (trials + 1) coarse steps, and by
+ * 5 * (trials + 1) more per variant when there are several. */
 OL_API int ol_ctx_autotune(ol_ctx *ctx, int32_t trials);
 /* ------------------------------------------------------------------ */
 /* Serving: continuous batching of solve requests over one context      */

@@ -212,6 +212,7 @@ _SIGS = {
     "ol_ctx_autotune": (C.c_int, [vp, i32]),
     "ol_ctx_set_launch": (C.c_int, [vp, i32]),
     "ol_ctx_get_launch": (C.c_int, [vp, C.POINTER(i32)]),
+    "ol_ctx_get_variant_launch": (C.c_int, [vp, i32, i32, i32, C.POINTER(i32)]),
     "ol_ctx_case_step": (C.c_int, [vp, i32, i32, f32]),
     "ol_ctx_case_coefficients": (C.c_int, [vp, i32, C.POINTER(CoeffRef), C.POINTER(C.c_double)]),
     "ol_set_stream_collide_kernel": (C.c_int, [i32, i32]),

@@ -21,6 +21,7 @@
 // step, so "old" f/vel are the other half of the A/B pair, and rho (a single
 // buffer in the reference) is kept as an A/B pair too.
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <map>
 #include <memory>
@@ -377,6 +378,10 @@ struct ol_ctx {
   // persistent kernel (cumulant without DDF; the other variants then take
   // one CTA per item)
   int grid_mult = -2;
+  // per collision variant [op][wale][ddf]: its own shape, or kShapeDefault
+  // to follow grid_mult (set by ol_ctx_autotune when the mix holds more than
+  // one variant)
+  int variant_shape[2][2][2] = {{{-99, -99}, {-99, -99}}, {{-99, -99}, {-99, -99}}};
   // >= 0: the plan holds this case only (ol_ctx_case_step), -1: every case
   int32_t only_case = -1;
   int64_t launches = 0;
@@ -519,6 +524,14 @@ static void free_plan(ol_ctx *c) {
 static int kernel_occupancy(int op) { return op == OL_OP_CUMULANT ? 2 : 1; }
 
 constexpr int kGridWs = -2;
+constexpr int kShapeDefault = -99;
+
+// Launch shape of a stream-collide launch group: its variant's own shape
+// when the autotuner set one, else the context's.
+static int shape_for(const ol_ctx *c, const Launch &l) {
+  const int s = c->variant_shape[l.op & 1][l.wale ? 1 : 0][l.ddf ? 1 : 0];
+  return s == kShapeDefault ? c->grid_mult : s;
+}
 
 template <int OP, class ST, bool WALE, bool DDF>
 static void launch_variant(ol_ctx *c, const Launch &l) {
@@ -529,7 +542,7 @@ static void launch_variant(ol_ctx *c, const Launch &l) {
     const int choice = stream_collide_kernel_choice();
     const bool f32 = std::is_same<ST, StoreF32>::value;
     if (choice == OL_SC_KERNEL_WS ||
-        (f32 && c->grid_mult == kGridWs && choice == OL_SC_KERNEL_AUTO)) {
+        (f32 && shape_for(c, l) == kGridWs && choice == OL_SC_KERNEL_AUTO)) {
       const int grid = ws_grid(l.n, c->n_sm);
       k_sc_ws<OP, ST, WALE, true><<<(unsigned)grid, kWsThreads, ws_smem_bytes<ST>(), c->stream>>>(
           LevelDev{}, c->d_descs, c->d_items + l.off, (int)l.n, ws_table_device(),
@@ -537,7 +550,8 @@ static void launch_variant(ol_ctx *c, const Launch &l) {
       return;
     }
   }
-  if (std::is_same<ST, StoreF32>::value && !DDF && c->grid_mult == -1) {
+  const int gm = shape_for(c, l);
+  if (std::is_same<ST, StoreF32>::value && !DDF && gm == -1) {
     // software-pipelined persistent kernel: all resident CTAs
     const int64_t grid = std::min<int64_t>(l.n, (int64_t)c->n_sm * kernel_occupancy(OP));
     k_sc_pipe<OP, WALE, true><<<(unsigned)grid, BCELLS, kPipeBytes, c->stream>>>(
@@ -545,7 +559,7 @@ static void launch_variant(ol_ctx *c, const Launch &l) {
     return;
   }
   const int64_t resident = (int64_t)c->n_sm * kernel_occupancy(OP);
-  int64_t grid = c->grid_mult <= 0 ? l.n : std::min<int64_t>(l.n, resident * c->grid_mult);
+  int64_t grid = gm <= 0 ? l.n : std::min<int64_t>(l.n, resident * gm);
   if (grid < 1) grid = 1;
   k_sc_batched<OP, ST, WALE, DDF><<<(unsigned)grid, BCELLS, kStageBytes, c->stream>>>(
       c->d_descs, c->d_tdescs, c->d_items + l.off, (int)l.n);
@@ -1331,6 +1345,9 @@ extern "C" int ol_ctx_set_launch(ol_ctx *c, int32_t shape) {
   OL_CHECK_ARG(shape >= OL_LAUNCH_WS && shape <= 2, "ol_ctx_set_launch: unknown shape %d", shape);
   std::lock_guard<std::mutex> lk(c->mu);
   c->grid_mult = shape;
+  for (auto &a : c->variant_shape)
+    for (auto &b : a)
+      for (auto &v : b) v = kShapeDefault;
   c->dirty = true;
   return OL_OK;
 }
@@ -1341,37 +1358,86 @@ extern "C" int ol_ctx_get_launch(ol_ctx *c, int32_t *shape) {
   return OL_OK;
 }
 
+extern "C" int ol_ctx_get_variant_launch(ol_ctx *c, int32_t op, int32_t wale, int32_t ddf,
+                                         int32_t *shape) {
+  OL_CHECK_ARG(c && shape, "ol_ctx_get_variant_launch: null argument");
+  OL_CHECK_ARG(op == OL_OP_CUMULANT || op == OL_OP_REGULARIZED_BGK,
+               "ol_ctx_get_variant_launch: unknown operator %d", op);
+  const int s = c->variant_shape[op][wale ? 1 : 0][ddf ? 1 : 0];
+  *shape = s == kShapeDefault ? c->grid_mult : s;
+  return OL_OK;
+}
+
+// Time `trials` coarse steps of the resident mix after one untimed step that
+// rebuilds the plan and graph under the shapes just set.
+static int time_mix(ol_ctx *c, int32_t trials, cudaEvent_t e0, cudaEvent_t e1, float *ms) {
+  int rc = ol_ctx_step(c, 1);
+  if (rc) return rc;
+  OL_CUDA(cudaEventRecord(e0, c->stream));
+  rc = ol_ctx_step(c, trials);
+  if (rc) return rc;
+  OL_CUDA(cudaEventRecord(e1, c->stream));
+  OL_CUDA(cudaEventSynchronize(e1));
+  OL_CUDA(cudaEventElapsedTime(ms, e0, e1));
+  return OL_OK;
+}
+
 extern "C" int ol_ctx_autotune(ol_ctx *c, int32_t trials) {
   OL_CHECK_ARG(c && trials > 0, "ol_ctx_autotune: bad argument");
   const int cands[5] = {OL_LAUNCH_WS, OL_LAUNCH_PER_ITEM, 1, 2, OL_LAUNCH_PIPELINED};
-  float best_ms = 1e30f;
-  int best = c->grid_mult;
   cudaEvent_t e0, e1;
   OL_CUDA(cudaEventCreate(&e0));
   OL_CUDA(cudaEventCreate(&e1));
-  for (int ci = 0; ci < 5; ++ci) {
-    {
-      std::lock_guard<std::mutex> lk(c->mu);
-      c->grid_mult = cands[ci];
-      c->dirty = true;
-    }
-    int rc = ol_ctx_step(c, 1);  // rebuild + warm
-    if (rc) return rc;
-    OL_CUDA(cudaEventRecord(e0, c->stream));
-    rc = ol_ctx_step(c, trials);
-    if (rc) return rc;
-    OL_CUDA(cudaEventRecord(e1, c->stream));
-    OL_CUDA(cudaEventSynchronize(e1));
+  auto set = [&](auto &&apply) {
+    std::lock_guard<std::mutex> lk(c->mu);
+    apply();
+    c->dirty = true;
+  };
+  auto reset_variants = [&]() {
+    for (auto &x : c->variant_shape)
+      for (auto &y : x)
+        for (auto &v : y) v = kShapeDefault;
+  };
+  // one shape for the whole mix
+  float best_ms = 1e30f;
+  int best = c->grid_mult;
+  int rc = OL_OK;
+  for (int ci = 0; ci < 5 && !rc; ++ci) {
+    set([&] { c->grid_mult = cands[ci]; reset_variants(); });
     float ms = 0.f;
-    OL_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-    if (ms < best_ms) { best_ms = ms; best = cands[ci]; }
+    rc = time_mix(c, trials, e0, e1, &ms);
+    if (!rc && ms < best_ms) { best_ms = ms; best = cands[ci]; }
+  }
+  if (!rc) set([&] { c->grid_mult = best; reset_variants(); });
+  // then, when the mix holds more than one collision variant, each variant's
+  // own shape with the others held (their time is the same in every trial)
+  std::vector<std::array<int, 3>> keys;
+  if (!rc) {
+    std::lock_guard<std::mutex> lk(c->mu);
+    for (const Launch &l : c->plan)
+      if (l.kind == 0) {
+        const std::array<int, 3> k{l.op & 1, l.wale ? 1 : 0, l.ddf ? 1 : 0};
+        if (std::find(keys.begin(), keys.end(), k) == keys.end()) keys.push_back(k);
+      }
+  }
+  if (keys.size() > 1) {
+    for (const auto &k : keys) {
+      int &slot = c->variant_shape[k[0]][k[1]][k[2]];
+      float kbest_ms = 1e30f;
+      int kbest = best;
+      for (int ci = 0; ci < 5 && !rc; ++ci) {
+        set([&] { slot = cands[ci]; });
+        float ms = 0.f;
+        rc = time_mix(c, trials, e0, e1, &ms);
+        if (!rc && ms < kbest_ms) { kbest_ms = ms; kbest = cands[ci]; }
+      }
+      if (rc) break;
+      set([&] { slot = kbest; });
+    }
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
-  std::lock_guard<std::mutex> lk(c->mu);
-  c->grid_mult = best;
-  c->dirty = true;
-  return OL_OK;
+  return rc;
 }
 
 extern "C" int ol_ctx_stats(ol_ctx *c, size_t *used, size_t *budget, int32_t *n_cases,

@@ -313,6 +313,13 @@ class Context:
         N.call("ol_ctx_get_launch", self._h, C.byref(out))
         return int(out.value)
 
+    def variant_launch(self, op: int, wale: bool, ddf: bool = False) -> int:
+        """Launch shape of one collision variant's stream-collide launches."""
+        out = C.c_int32()
+        N.call("ol_ctx_get_variant_launch", self._h, op, int(bool(wale)), int(bool(ddf)),
+               C.byref(out))
+        return int(out.value)
+
     def stats(self) -> dict:
         used, budget = C.c_size_t(), C.c_size_t()
         n, launches = C.c_int32(), C.c_int64()

@@ -237,3 +237,30 @@ def test_autotune_keeps_results_valid(one_level):
     f_ref = ref.download(rid, 1, f=True)[2]
     ref.close()
     assert rel_err(f_tuned, f_ref) < 1e-6
+
+
+def test_autotune_per_variant_on_a_two_variant_mix(one_level, two_level):
+    """A mix of a case without WALE and one with it holds two collision
+    variants: the tuner times the whole mix, then each variant's shape with
+    the other held, and every case steps 5 * 2 + 2 * 5 * 2 = 30 coarse steps
+    (trials = 1).  The state it leaves is that of the same steps under one
+    CTA per item."""
+    ctx = NT.Context(budget_bytes=2 << 30, storage="f32")
+    ids = [ctx.add_case(c) for c in (one_level, two_level)]
+    ctx.autotune(1)
+    shapes = {w: ctx.variant_launch(0, w) for w in (False, True)}
+    assert all(v in SHAPES.values() for v in shapes.values())
+    assert [ctx.info(i) for i in ids] == [(30, 0), (30, 0)]
+    got = [ctx.download(i, lvl, f=True)[2] for i, c in zip(ids, (one_level, two_level))
+           for lvl in range(1, len(c.levels) + 1)]
+    ctx.close()
+    ref = NT.Context(budget_bytes=2 << 30, storage="f32")
+    rids = [ref.add_case(c) for c in (one_level, two_level)]
+    ref.set_launch(0)
+    assert ref.variant_launch(0, True) == 0
+    ref.step(30)
+    want = [ref.download(i, lvl, f=True)[2] for i, c in zip(rids, (one_level, two_level))
+            for lvl in range(1, len(c.levels) + 1)]
+    ref.close()
+    for g, w in zip(got, want):
+        assert rel_err(g, w) < 1e-6
