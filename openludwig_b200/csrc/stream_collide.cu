@@ -88,6 +88,12 @@ static std::vector<uint32_t> build_ws_table() {
           if (on) tab.push_back(dir | (uint32_t)(x + 8 * y + 64 * z) << 5);
         }
   }
+  // the FP32 compute-stage slot of each out-of-block pull
+  for (int i = 0; i < kHaloEntries; ++i) {
+    const uint32_t e = tab[i];
+    const int k = e & 31, d = (int)(e >> 19);
+    tab.push_back((uint32_t)(k * kSPlane + kSPad + d - cx_of(k)));
+  }
   return tab;
 }
 
@@ -99,7 +105,7 @@ const uint32_t *ws_table_device() {
   std::lock_guard<std::mutex> lk(mu);
   if (!per_dev[dev]) {
     const std::vector<uint32_t> tab = build_ws_table();
-    if ((int)tab.size() != kWsTableSize) return nullptr;
+    if ((int)tab.size() != kWsTableTotal) return nullptr;
     uint32_t *d = nullptr;
     if (cudaMalloc(&d, tab.size() * sizeof(uint32_t)) != cudaSuccess) return nullptr;
     if (cudaMemcpy(d, tab.data(), tab.size() * sizeof(uint32_t), cudaMemcpyHostToDevice) !=

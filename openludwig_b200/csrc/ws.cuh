@@ -55,6 +55,10 @@ constexpr int kWsRing = 4;  // descriptor / neighbour-offset slots (item j uses 
 // (face dir | own cell beside the slot << 5).
 constexpr int kWsVelEntries = 6 * 64;
 constexpr int kWsTableSize = kHaloEntries + kWsVelEntries;
+// ... then, per out-of-block pull i, the index of the FP32 compute-stage slot
+// it is written to (k * kSPlane + kSPad + destination cell - c_x(k); below)
+constexpr int kWsSlotOffset = kWsTableSize;
+constexpr int kWsTableTotal = kWsTableSize + kHaloEntries;
 // Dynamic shared memory (byte offsets).
 // FP32 storage ("direct"): the bulk copies land each population plane k
 // straight into the compute stage, shifted by 8 c_y + 64 c_z cells, so the
@@ -80,8 +84,8 @@ template <> struct WsLayout<StoreF32> {
   static constexpr int kLdSP = kLdV + 3 * BCELLS * 4;           // float [512]
   static constexpr int kLdWD = kLdSP + BCELLS * 4;              // float [512]
   static constexpr int kLdOB = kLdWD + BCELLS * 4;              // uint8 [512]
-  static constexpr int kTab = kLdOB + BCELLS;                   // uint32 [kWsTableSize]
-  static constexpr int kBytes = kTab + kWsTableSize * 4;        // 107,840
+  static constexpr int kTab = kLdOB + BCELLS;                   // uint32 [kWsTableTotal]
+  static constexpr int kBytes = kTab + kWsTableTotal * 4;       // 120,544
   static constexpr int kLdF = 0, kF = 0;                        // (unused)
 };
 template <> struct WsLayout<StoreF16S> {
@@ -93,8 +97,8 @@ template <> struct WsLayout<StoreF16S> {
   static constexpr int kLdOB = kLdWD + BCELLS * 4;              // uint8 [512]
   static constexpr int kF = kLdOB + BCELLS;                     // float [27][512], pre-streamed
   static constexpr int kV = kF + 27 * BCELLS * 4;               // float [3][1000]
-  static constexpr int kTab = kV + 3 * EPL * 4;                 // uint32 [kWsTableSize]
-  static constexpr int kBytes = kTab + kWsTableSize * 4;        // 147,584
+  static constexpr int kTab = kV + 3 * EPL * 4;                 // uint32 [kWsTableTotal]
+  static constexpr int kBytes = kTab + kWsTableTotal * 4;       // 160,288
   static constexpr int kS = 0;                                  // (unused)
 };
 static_assert(WsLayout<StoreF32>::kV % 16 == 0 && WsLayout<StoreF32>::kLdV % 16 == 0 &&
@@ -319,7 +323,7 @@ __global__ void __launch_bounds__(kWsThreads, 1)
     mbar_init(lfree, BCELLS / 32);  // one arrival per consumer warp
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  for (int i = t; i < kWsTableSize; i += kWsThreads) tabs[i] = __ldg(tab + i);
+  for (int i = t; i < kWsTableTotal; i += kWsThreads) tabs[i] = __ldg(tab + i);
   __syncthreads();
   pdl_wait();  // f_in, vel_in, ghost rows: written by the launches before this one
 
@@ -401,7 +405,7 @@ __global__ void __launch_bounds__(kWsThreads, 1)
       const float v = (nbase[dir] >= 0 || ghost)
                           ? h.f[m]
                           : pull_boundary<ST>(L, k, b, d & 7, (d >> 3) & 7, d >> 6);
-      if constexpr (Lay::kDirect) F[k * kSPlane + kSPad + d - cx_of(k)] = v;
+      if constexpr (Lay::kDirect) F[tabs[kWsSlotOffset + i]] = v;
       else F[k * BCELLS + d] = v;
     }
     if (WALE) {
