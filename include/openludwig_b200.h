@@ -168,6 +168,16 @@ OL_API int ol_set_stream_collide_kernel(int32_t choice, int32_t max_ctas);
  * the kernel then ends early and its output is incomplete).  0 = none. */
 OL_API int ol_pipeline_fault(int32_t *flags);
 
+/* Host copies of the static staging tables (no GPU needed; for checking the
+ * kernels' index arithmetic): the staging table of the one-CTA-per-block
+ * kernel and the ghost pass, and the loader table of the warp-specialised
+ * kernel (out-of-block pulls k | dir << 5 | source cell << 10 | pulling cell
+ * << 19, face-halo velocity slots, then the FP32 stage slot of each pull).
+ * sizes[4] = {halo entries, loader entries, stage plane slots, stage pad}; a
+ * table is copied when its buffer is non-NULL and large enough. */
+OL_API int ol_staging_tables(uint32_t *halo, int32_t halo_cap, uint32_t *ws, int32_t ws_cap,
+                             int32_t *sizes);
+
 /* Bouzidi interpolated bounce-back (bouzidi_kernel.jl:13-122).  q_map holds
  * IEEE binary16 bit patterns [512*nB*27]; cell_* are the sparse boundary-cell
  * lists (block 1-based Int32, x/y/z 1-based Int8).  Reads f_post, writes f_out. */

@@ -217,6 +217,7 @@ _SIGS = {
     "ol_ctx_case_coefficients": (C.c_int, [vp, i32, C.POINTER(CoeffRef), C.POINTER(C.c_double)]),
     "ol_set_stream_collide_kernel": (C.c_int, [i32, i32]),
     "ol_pipeline_fault": (C.c_int, [C.POINTER(i32)]),
+    "ol_staging_tables": (C.c_int, [vp, i32, vp, i32, C.POINTER(i32)]),
     "ol_server_create": (C.c_int, [C.POINTER(vp), vp, C.POINTER(ServeRule)]),
     "ol_server_destroy": (C.c_int, [vp]),
     "ol_server_clock": (C.c_int, [vp, C.POINTER(C.c_double)]),

@@ -1,5 +1,6 @@
 // Drop-in stream-collide launch: one CTA per 8^3 block, one thread per cell,
 // caller buffers in the reference layout (FP32 populations).
+#include <algorithm>
 #include <cstdlib>
 #include <mutex>
 #include <type_traits>
@@ -426,6 +427,19 @@ extern "C" int ol_pipeline_fault(int32_t *flags) {
   OL_CUDA(cudaMemcpy(&v, d, sizeof(int), cudaMemcpyDeviceToHost));
   OL_CUDA(cudaMemset(d, 0, sizeof(int)));
   *flags = v;
+  return OL_OK;
+}
+
+extern "C" int ol_staging_tables(uint32_t *halo, int32_t halo_cap, uint32_t *ws, int32_t ws_cap,
+                                 int32_t *sizes) {
+  OL_CHECK_ARG(sizes, "ol_staging_tables: null sizes");
+  const std::vector<uint32_t> h = build_halo_table(), w = build_ws_table();
+  sizes[0] = (int32_t)h.size();
+  sizes[1] = (int32_t)w.size();
+  sizes[2] = kSPlane;
+  sizes[3] = kSPad;
+  if (halo && halo_cap >= (int32_t)h.size()) std::copy(h.begin(), h.end(), halo);
+  if (ws && ws_cap >= (int32_t)w.size()) std::copy(w.begin(), w.end(), ws);
   return OL_OK;
 }
 
