@@ -1,6 +1,10 @@
 // Thermal DDF launch and its C ABI (stream_collide_thermal!, timestep.jl:101-145).
+#include <cstdint>
+#include <type_traits>
+
 #include "common.cuh"
 #include "thermal.cuh"
+#include "thermal_ws.cuh"
 
 namespace ol {
 
@@ -24,15 +28,50 @@ __global__ void __launch_bounds__(kGhostThreads, kGhostMinBlocks)
   ghost_fill_block<ST>(D, b, ghost_row_of(D, b), ghost_next_row_of(D, b));
 }
 
+static int sm_count() {
+  static int n_sm[64] = {};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 148;
+  if (!n_sm[dev]) {
+    int v = 0;
+    if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || v <= 0)
+      v = 148;
+    n_sm[dev] = v;
+  }
+  return n_sm[dev];
+}
+
+// Whether the warp-specialised thermal kernel serves this FP32 level: chosen
+// (forced, or by default on levels of at least two blocks per SM); every
+// absent-neighbour value precomputed in ghost rows or a level-1
+// domain-boundary value; the arrays it bulk-copies 16-byte aligned.
+static bool thermal_ws_applies(const ThermalDev &D, int n_sm) {
+  auto a16 = [](const void *p) { return ((uintptr_t)p & 15) == 0; };
+  const int choice = stream_collide_kernel_choice();
+  if (!(choice == OL_SC_KERNEL_WS || (choice == OL_SC_KERNEL_AUTO && D.n_blocks >= 2 * n_sm)))
+    return false;
+  if (!D.tp.is_level_1 && !D.ghost) return false;
+  if (!a16(D.g_in) || !a16(D.vel) || !a16(D.sponge) || !a16(D.obstacle)) return false;
+  return fault_word_device() != nullptr && ws_table_device() != nullptr;
+}
+
 template <class ST>
 static void launch_t(const ThermalDev &D, cudaStream_t s) {
   static bool done = false;
   if (!done) {
     cudaFuncSetAttribute(k_thermal<ST>, cudaFuncAttributeMaxDynamicSharedMemorySize, kStageBytes);
+    if (std::is_same<ST, StoreF32>::value)
+      cudaFuncSetAttribute(k_thermal_ws, cudaFuncAttributeMaxDynamicSharedMemorySize, kTwBytes);
     done = true;
   }
   const int gn = D.gblocks ? D.n_gblocks : D.n_blocks;
   if (D.ghost && gn > 0) k_ghost_fill_thermal<ST><<<gn, kGhostThreads, 0, s>>>(D);
+  const int n_sm = sm_count();
+  if (std::is_same<ST, StoreF32>::value && thermal_ws_applies(D, n_sm)) {
+    k_thermal_ws<<<ws_grid(D.n_blocks, n_sm), kWsThreads, kTwBytes, s>>>(D, ws_table_device(),
+                                                                         fault_word_device());
+    return;
+  }
   k_thermal<ST><<<D.n_blocks, BCELLS, kStageBytes, s>>>(D);
 }
 

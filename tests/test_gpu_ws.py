@@ -186,3 +186,32 @@ def test_ws_block_pool_equals_block_kernel(storage):
         ctx.close()
     for x, y in zip(*out):
         assert rel_err(y, x) < 1e-6
+
+
+@pytest.mark.parametrize("max_ctas", [0, 13], ids=["cta_per_sm", "13_ctas"])
+def test_thermal_ws_equals_block_kernel(max_ctas):
+    """The warp-specialised thermal kernel (bulk-copied g planes landing in
+    the pull-shifted stage) against the one-CTA-per-block thermal kernel on a
+    two-level O(u^4) + DDF sphere (ghost rows on the refined level, domain
+    boundaries on level 1, solid cells bouncing their own g), 4 coarse steps:
+    f, g, rho, T and u of both levels within 1e-6 relative L2."""
+    c, mesh, p, hosts = small_sphere_case(resolution=16, levels=2, c_wale=np.float32(0.5),
+                                          compressibility_correction=True, ddf_enabled=True,
+                                          u_target=np.float32(0.1))
+    st = S.StepSettings.from_config(c, False)
+    dims = (p.nx_coarse, p.ny_coarse, p.nz_coarse)
+
+    def run(choice, ctas):
+        _kernel(choice, ctas)
+        levels = [S.upload_level(h, DEV, ddf=True, t_init=c.ddf_t_initial) for h in hosts]
+        for t in range(1, 5):
+            S.recursive_step(levels, st, 0, t, None, 0.0, 0.1, dims)
+        torch.cuda.synchronize()
+        return levels
+
+    a = run(BLOCK, 0)
+    b = run(WS, max_ctas)
+    for la, lb in zip(a, b):
+        for name in ("f", "f_temp", "g", "g_temp", "rho", "temperature", "vel", "vel_temp"):
+            x, y = getattr(la, name).cpu().numpy(), getattr(lb, name).cpu().numpy()
+            assert rel_err(y, x) < 1e-6, name
