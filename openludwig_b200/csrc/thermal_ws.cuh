@@ -21,14 +21,18 @@
 
 namespace ol {
 
-// Dynamic shared memory (bytes).
+// Dynamic shared memory (bytes): two buffers, so that two blocks are in
+// flight per SM (the update is too short to hide one block's copies), each
+// a stage with the velocity, sponge and mask beside it; then the table.
 constexpr int kTwS = 0;                                // float [27][kSPlane]
 constexpr int kTwLdV = kTwS + 27 * kSPlane * 4;        // float [3][512] flow velocity
 constexpr int kTwLdSP = kTwLdV + 3 * BCELLS * 4;       // float [512]
 constexpr int kTwLdOB = kTwLdSP + BCELLS * 4;          // uint8 [512]
-constexpr int kTwTab = kTwLdOB + BCELLS;               // uint32 [kWsTableTotal]
-constexpr int kTwBytes = kTwTab + kWsTableTotal * 4;   // 106,496
-static_assert(kTwLdV % 16 == 0 && kTwLdSP % 16 == 0 && kTwLdOB % 16 == 0 && kTwTab % 16 == 0,
+constexpr int kTwBuf = kTwLdOB + BCELLS;               // bytes per buffer (79,552)
+constexpr int kTwTab = 2 * kTwBuf;                     // uint32 [kWsTableTotal]
+constexpr int kTwBytes = kTwTab + kWsTableTotal * 4;   // 186,048
+constexpr int kTwRing = 8;                             // descriptor slots (block j uses j & 7)
+static_assert(kTwLdV % 16 == 0 && kTwLdSP % 16 == 0 && kTwLdOB % 16 == 0 && kTwBuf % 16 == 0,
               "bulk-copy destinations stay 16-byte aligned");
 
 // The producer's bulk copies of block b into the stage (lane 0 announces the
@@ -133,18 +137,26 @@ __global__ void __launch_bounds__(kWsThreads, 1)
     k_thermal_ws(const __grid_constant__ ThermalDev D, const uint32_t *__restrict__ tab,
                  int *fault) {
   extern __shared__ __align__(16) unsigned char tw_smem[];
-  __shared__ int nbb[kWsRing][27];
-  __shared__ int blk[kWsRing];
-  __shared__ __align__(8) uint64_t bars[2];  // landed, free
-  uint64_t *const landed = &bars[0], *const lfree = &bars[1];
+  // neighbour offsets and block of block p in slot p & (kTwRing - 1): the
+  // producer fetches block j+1 before waiting for buffer j & 1, while the
+  // consumers may still be finishing block j-3
+  __shared__ int nbb[kTwRing][27];
+  __shared__ int blk[kTwRing];
+  // per buffer: "landed" (bulk bytes plus the producer's arrival), "free"
+  // (one arrival per consumer warp); block j uses buffer j & 1, and its
+  // (j >> 1)-th phase of each
+  __shared__ __align__(8) uint64_t bars[4];
+  uint64_t *const landed = &bars[0], *const lfree = &bars[2];
   uint32_t *const tabs = (uint32_t *)(tw_smem + kTwTab);
   const int t = threadIdx.x;
   const int n = D.n_blocks;
   const int first = blockIdx.x;
   const int cnt = first < n ? (n - 1 - first) / (int)gridDim.x + 1 : 0;
   if (t == 0) {
-    mbar_init(landed, 1);
-    mbar_init(lfree, BCELLS / 32);
+    for (int i = 0; i < 2; ++i) {
+      mbar_init(landed + i, 1);
+      mbar_init(lfree + i, BCELLS / 32);
+    }
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   for (int i = t; i < kWsTableTotal; i += kWsThreads) tabs[i] = __ldg(tab + i);
@@ -154,7 +166,7 @@ __global__ void __launch_bounds__(kWsThreads, 1)
     // ------------------------------------------------------------ producer
     const int lane = t - BCELLS;
     auto fetch = [&](int p) {
-      const int r = p & (kWsRing - 1);
+      const int r = p & (kTwRing - 1);
       const int b = first + p * (int)gridDim.x;
       if (lane < 27) {
         const int nb = D.nbr[b + D.nbr_stride * lane];
@@ -167,28 +179,29 @@ __global__ void __launch_bounds__(kWsThreads, 1)
     if (cnt > 1) fetch(1);
     int j = 0;
     for (; j < cnt; ++j) {
-      const int r = j & (kWsRing - 1);
+      const int r = j & (kTwRing - 1), bi = j & 1;
       if (j >= 1 && j + 1 < cnt) fetch(j + 1);
-      // the stage is free once the consumers have pulled block j-1
-      const bool ok = j == 0 || mbar_wait(lfree, (j - 1) & 1, fault, kWsFaultLoaderWait);
+      // buffer bi is free once the consumers have pulled block j-2
+      const bool ok =
+          j < 2 || mbar_wait(lfree + bi, ((j - 2) >> 1) & 1, fault, kWsFaultLoaderWait);
       if (!__all_sync(0xffffffffu, ok)) break;
-      if (j > 0) asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-      tws_produce(D, blk[r], lane, tw_smem, landed);
+      if (j >= 2) asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      tws_produce(D, blk[r], lane, tw_smem + bi * kTwBuf, landed + bi);
     }
     // bulk copies still in flight (a loop left early) land before the CTA exits
-    if (j > 0 && j < cnt) mbar_wait(landed, (j - 1) & 1, nullptr, 0);
+    if (j < cnt)
+      for (int i = j >= 2 ? j - 2 : 0; i < j; ++i)
+        mbar_wait(landed + (i & 1), (i >> 1) & 1, nullptr, 0);
     return;
   }
 
   // -------------------------------------------------------------- consumers
-  float *const F = (float *)(tw_smem + kTwS);
-  const float *const lv = (const float *)(tw_smem + kTwLdV);
-  const float *const lsp = (const float *)(tw_smem + kTwLdSP);
-  const uint8_t *const lob = tw_smem + kTwLdOB;
   float h[kWsHaloPerConsumer];
   for (int j = 0; j < cnt; ++j) {
-    const int r = j & (kWsRing - 1);
-    const bool ok = mbar_wait(landed, j & 1, fault, kWsFaultConsumerWait);
+    const int r = j & (kTwRing - 1), bi = j & 1;
+    unsigned char *const buf = tw_smem + bi * kTwBuf;
+    float *const F = (float *)(buf + kTwS);
+    const bool ok = mbar_wait(landed + bi, (j >> 1) & 1, fault, kWsFaultConsumerWait);
     if (!consumer_sync_and(ok)) break;  // also: every consumer is done pulling block j-1
     const int *nbase = nbb[r];
     const int b = blk[r];
@@ -205,19 +218,20 @@ __global__ void __launch_bounds__(kWsThreads, 1)
                           : pull_boundary_thermal<StoreF32>(D, k, b, d & 7, (d >> 3) & 7, d >> 6);
       F[tabs[kWsSlotOffset + i]] = v;
     }
+    const float *const lv = (const float *)(buf + kTwLdV);
     const float ux = lv[t], uy = lv[BCELLS + t], uz = lv[2 * BCELLS + t];
-    const float spg = lsp[t];
-    const bool obs = lob[t] != 0;
+    const float spg = ((const float *)(buf + kTwLdSP))[t];
+    const bool obs = buf[kTwLdOB + t] != 0;
     consumer_sync();  // the stage holds block j
     float A[27];
 #pragma unroll
     for (int k = 0; k < 27; ++k) A[k] = F[k * kSPlane + kSPad + t - cx_of(k)];
-    // the stage is read: order these accesses before the next bulk copies
+    // the buffer is read: order these accesses before its next bulk copies
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncwarp();
+    if ((t & 31) == 0) mbar_arrive(lfree + bi);
     if (j + 1 < cnt) {
-      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-      __syncwarp();
-      if ((t & 31) == 0) mbar_arrive(lfree);
-      const int r1 = (j + 1) & (kWsRing - 1);
+      const int r1 = (j + 1) & (kTwRing - 1);
       tws_halo_load(D, blk[r1], nbb[r1], t, tabs, h);
     }
     tws_cell(D, (size_t)nbase[13] + t, A, ux, uy, uz, spg, obs);
