@@ -188,13 +188,15 @@ def test_ws_block_pool_equals_block_kernel(storage):
         assert rel_err(y, x) < 1e-6
 
 
-@pytest.mark.parametrize("max_ctas", [0, 13], ids=["cta_per_sm", "13_ctas"])
+@pytest.mark.parametrize("max_ctas", [0, 13, 3], ids=["cta_per_sm", "13_ctas", "3_ctas"])
 def test_thermal_ws_equals_block_kernel(max_ctas):
     """The warp-specialised thermal kernel (bulk-copied g planes landing in
     the pull-shifted stage) against the one-CTA-per-block thermal kernel on a
     two-level O(u^4) + DDF sphere (ghost rows on the refined level, domain
     boundaries on level 1, solid cells bouncing their own g), 4 coarse steps:
-    f, g, rho, T and u of both levels within 1e-6 relative L2."""
+    f, g, rho, T and u of both levels within 1e-6 relative L2.  With 3 CTAs
+    each walks dozens of blocks, so the producer's look-ahead (two stage
+    buffers, descriptors of the next block) runs well ahead of the consumers."""
     c, mesh, p, hosts = small_sphere_case(resolution=16, levels=2, c_wale=np.float32(0.5),
                                           compressibility_correction=True, ddf_enabled=True,
                                           u_target=np.float32(0.1))
