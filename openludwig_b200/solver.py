@@ -162,10 +162,20 @@ def upload_level(h: HostLevel, device: torch.device, ddf: bool = False, t_init: 
     return lv
 
 
+# Out-of-block pulls a block makes from its neighbour in direction d: 484
+# from a face neighbour (22 x 22 cell-direction pairs), 22 from an edge, 1
+# from a corner (3176 in all).
+_PULLS_FROM_NEIGHBOUR = np.array(
+    [{0: 0, 1: 484, 2: 22, 3: 1}[abs(d % 3 - 1) + abs((d // 3) % 3 - 1) + abs(d // 9 - 1)]
+     for d in range(27)], dtype=np.int64)
+
+
 def ghost_block_lists(h: HostLevel, dims) -> tuple[np.ndarray, np.ndarray]:
     """0-based ids (int32) of the blocks with an absent neighbour, and of
     those with an absent neighbour block not wholly inside the level's
-    domain (dims = its size in cells): the ghost pass's visit lists."""
+    domain (dims = its size in cells): the ghost pass's visit lists.  Each
+    list is ordered by the number of absent-neighbour pulls, largest first
+    (ties by block id), so the pass's last CTAs are its shortest ones."""
     n = h.n_blocks
     missing = np.asarray(h.neighbor_table).reshape(27, n) <= 0     # [dir, block]
     d = np.arange(27)
@@ -174,9 +184,13 @@ def ghost_block_lists(h: HostLevel, dims) -> tuple[np.ndarray, np.ndarray]:
                        (h.map_z, d // 9 - 1, dims[2])):
         c = np.asarray(m, dtype=np.int64)[None, :] + off[:, None]
         inside &= (c >= 1) & (c * BS <= nc)
-    ghost = np.nonzero(missing.any(axis=0))[0].astype(np.int32)
-    edge = np.nonzero((missing & ~inside).any(axis=0))[0].astype(np.int32)
-    return ghost, edge
+
+    def by_work(sel):
+        ids = np.nonzero(sel.any(axis=0))[0]
+        work = (sel[:, ids] * _PULLS_FROM_NEIGHBOUR[:, None]).sum(axis=0)
+        return ids[np.argsort(-work, kind="stable")].astype(np.int32)
+
+    return by_work(missing), by_work(missing & ~inside)
 
 
 def lattice_weights() -> list:
