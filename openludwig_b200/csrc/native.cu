@@ -23,10 +23,12 @@
 #include <algorithm>
 #include <array>
 #include <cmath>
+#include <cstdlib>
 #include <map>
 #include <memory>
 #include <mutex>
 #include <type_traits>
+#include <utility>
 #include <vector>
 
 #include "batched.cuh"
@@ -280,41 +282,67 @@ struct DevLevel {
   int32_t *gidx = nullptr;
   std::vector<int32_t> ghost_blocks;  // host copy of the blocks with a row
   std::vector<int32_t> edge_blocks;   // those of them with domain-boundary values
+  std::vector<int32_t> ghost_work;    // absent-neighbour pulls of each, in list order
+  std::vector<int32_t> edge_work;     // domain-boundary pulls of each edge block
 };
 
-// Blocks of a level with at least one absent neighbour (neighbour table
-// nB x 27 column-major, 0 = absent).
-static std::vector<int32_t> blocks_with_absent_neighbour(const ol_level_desc &S) {
-  std::vector<int32_t> out;
-  for (int b = 0; b < S.n_blocks; ++b)
-    for (int d = 0; d < 27; ++d)
-      if (S.neighbor_table[b + (size_t)S.n_blocks * d] <= 0) {
-        out.push_back(b);
-        break;
-      }
-  return out;
+// Out-of-block pulls a block makes from its neighbour in direction d: 484
+// from a face neighbour, 22 from an edge, 1 from a corner (3176 in all).
+static int pulls_from_neighbour(int d) {
+  const int m = std::abs(d % 3 - 1) + std::abs((d / 3) % 3 - 1) + std::abs(d / 9 - 1);
+  return m == 1 ? 484 : m == 2 ? 22 : m == 3 ? 1 : 0;
 }
 
-// Of `ghost`, the blocks with an absent neighbour not wholly inside the
-// level's domain (n*_global cells per axis): the only blocks whose values
-// the second sub-step of a pair evaluates (domain boundary conditions); every
-// other absent-neighbour value is coarse-to-fine and set by the first.
-static std::vector<int32_t> blocks_with_domain_edge(const ol_level_desc &S,
-                                                    const std::vector<int32_t> &ghost, int nxg,
-                                                    int nyg, int nzg) {
-  std::vector<int32_t> out;
+// The blocks with a nonzero work[b], largest first (ties by block id), and
+// their work in that order: the ghost pass's visit order, so that its last
+// CTAs are its shortest ones.
+static void order_by_work(const std::vector<int32_t> &work, std::vector<int32_t> &blocks,
+                          std::vector<int32_t> &sorted_work) {
+  blocks.clear();
+  for (int b = 0; b < (int)work.size(); ++b)
+    if (work[b] > 0) blocks.push_back(b);
+  std::stable_sort(blocks.begin(), blocks.end(),
+                   [&](int32_t a, int32_t b) { return work[a] > work[b]; });
+  sorted_work.clear();
+  for (int32_t b : blocks) sorted_work.push_back(work[b]);
+}
+
+// Blocks of a level with at least one absent neighbour (neighbour table
+// nB x 27 column-major, 0 = absent), by absent-neighbour pulls.
+static void blocks_with_absent_neighbour(const ol_level_desc &S, std::vector<int32_t> &blocks,
+                                         std::vector<int32_t> &work_out) {
+  std::vector<int32_t> work((size_t)S.n_blocks, 0);
+  for (int b = 0; b < S.n_blocks; ++b)
+    for (int d = 0; d < 27; ++d)
+      if (d != 13 && S.neighbor_table[b + (size_t)S.n_blocks * d] <= 0)
+        work[b] += pulls_from_neighbour(d);
+  order_by_work(work, blocks, work_out);
+}
+static size_t count_blocks_with_absent_neighbour(const ol_level_desc &S) {
+  std::vector<int32_t> blocks, work;
+  blocks_with_absent_neighbour(S, blocks, work);
+  return blocks.size();
+}
+
+// The blocks with an absent neighbour not wholly inside the level's domain
+// (n*_global cells per axis), by their pulls from such neighbours: the only
+// blocks whose values the second sub-step of a pair evaluates (domain
+// boundary conditions); every other absent-neighbour value is coarse-to-fine
+// and set by the first.
+static void blocks_with_domain_edge(const ol_level_desc &S, int nxg, int nyg, int nzg,
+                                    std::vector<int32_t> &blocks,
+                                    std::vector<int32_t> &work_out) {
   auto inside = [](int nb, int ng) { return nb >= 1 && (int64_t)nb * BS <= ng; };
-  for (int32_t b : ghost)
+  std::vector<int32_t> work((size_t)S.n_blocks, 0);
+  for (int b = 0; b < S.n_blocks; ++b)
     for (int d = 0; d < 27; ++d) {
-      if (S.neighbor_table[b + (size_t)S.n_blocks * d] > 0) continue;
+      if (d == 13 || S.neighbor_table[b + (size_t)S.n_blocks * d] > 0) continue;
       const int nbx = S.map_x[b] + d % 3 - 1, nby = S.map_y[b] + (d / 3) % 3 - 1,
                 nbz = S.map_z[b] + d / 9 - 1;
-      if (!inside(nbx, nxg) || !inside(nby, nyg) || !inside(nbz, nzg)) {
-        out.push_back(b);
-        break;
-      }
+      if (!inside(nbx, nxg) || !inside(nby, nyg) || !inside(nbz, nzg))
+        work[b] += pulls_from_neighbour(d);
     }
-  return out;
+  order_by_work(work, blocks, work_out);
 }
 
 struct NCase {
@@ -453,7 +481,7 @@ static size_t case_meta_bytes(const ol_case_desc *cd) {
       b += cut_links(L, cd->q_min_threshold > 0.0f ? cd->q_min_threshold : 0.001f).size() *
            sizeof(ol_bouzidi_link);
     if (l > 0)  // ghost rows of both sub-steps of a pair, flow (+ thermal)
-      b += blocks_with_absent_neighbour(L).size() * kHaloEntries * sizeof(float) * 2 *
+      b += count_blocks_with_absent_neighbour(L) * kHaloEntries * sizeof(float) * 2 *
                (cd->ddf ? 2 : 1) +
            (size_t)L.n_blocks * sizeof(int32_t);
   }
@@ -660,7 +688,8 @@ static int rebuild(ol_ctx *c) {
     std::map<int, std::vector<int>> groups;  // variant -> descriptor ids
     int64_t scratch_off = 0;
     std::vector<int> bz_flow, bz_therm;
-    std::vector<WorkItem> ghost_items, tghost_items;
+    // (work, item): each ghost launch visits the blocks of all cases largest first
+    std::vector<std::pair<int32_t, WorkItem>> ghost_items, tghost_items;
     for (auto &kv : c->cases) {
       NCase &cs = *kv.second;
       if (c->only_case >= 0 && kv.first != c->only_case) continue;
@@ -698,8 +727,9 @@ static int rebuild(ol_ctx *c) {
         L.ghost_next = V.ghost2;
         L.ghost_mode = first ? kGhostPairFirst : kGhostPairSecond;
         L.gidx = V.gidx;
-        for (int32_t b : first ? V.ghost_blocks : V.edge_blocks)
-          ghost_items.push_back(WorkItem{d, b});
+        const auto &gb = first ? V.ghost_blocks : V.edge_blocks;
+        const auto &gw = first ? V.ghost_work : V.edge_work;
+        for (size_t q = 0; q < gb.size(); ++q) ghost_items.push_back({gw[q], WorkItem{d, gb[q]}});
       } else {
         L.sp.tau_parent = 0.5f;
         L.p_inv_scale = 1.0f;
@@ -727,8 +757,10 @@ static int rebuild(ol_ctx *c) {
           D.ghost_next = V.ghost_g2;
           D.ghost_mode = first ? kGhostPairFirst : kGhostPairSecond;
           D.gidx = V.gidx;
-          for (int32_t b : first ? V.ghost_blocks : V.edge_blocks)
-            tghost_items.push_back(WorkItem{d, b});
+          const auto &gb = first ? V.ghost_blocks : V.edge_blocks;
+          const auto &gw = first ? V.ghost_work : V.edge_work;
+          for (size_t q = 0; q < gb.size(); ++q)
+            tghost_items.push_back({gw[q], WorkItem{d, gb[q]}});
         } else {
           D.tp.tau_g_parent = 0.5f;
           D.p_inv_scale = 1.0f;
@@ -763,24 +795,21 @@ static int rebuild(ol_ctx *c) {
         }
       }
     }
-    if (!ghost_items.empty()) {  // boundary values of the refined levels first
+    auto ghost_launch = [&](std::vector<std::pair<int32_t, WorkItem>> &gi, int kind) {
+      if (gi.empty()) return;
+      std::stable_sort(gi.begin(), gi.end(),
+                       [](const std::pair<int32_t, WorkItem> &a,
+                          const std::pair<int32_t, WorkItem> &b) { return a.first > b.first; });
       Launch gl{};
-      gl.kind = 3;
+      gl.kind = kind;
       gl.off = (int64_t)items.size();
-      items.insert(items.end(), ghost_items.begin(), ghost_items.end());
-      gl.n = (int64_t)ghost_items.size();
+      for (const auto &w : gi) items.push_back(w.second);
+      gl.n = (int64_t)gi.size();
       c->plan.push_back(gl);
       ++per_step;
-    }
-    if (!tghost_items.empty()) {  // and of the thermal populations of DDF cases
-      Launch gl{};
-      gl.kind = 4;
-      gl.off = (int64_t)items.size();
-      items.insert(items.end(), tghost_items.begin(), tghost_items.end());
-      gl.n = (int64_t)tghost_items.size();
-      c->plan.push_back(gl);
-      ++per_step;
-    }
+    };
+    ghost_launch(ghost_items, 3);   // boundary values of the refined levels first
+    ghost_launch(tghost_items, 4);  // and of the thermal populations of DDF cases
     for (auto &g : groups) {
       Launch ln{};
       ln.kind = 0;
@@ -1010,13 +1039,13 @@ extern "C" int ol_ctx_case_add(ol_ctx *c, const ol_case_desc *cd, int32_t *case_
       OL_CUDA(cudaMemcpy(c->wd + c0, far.data(), nc * 4, cudaMemcpyHostToDevice));
     }
     if (l > 0) {
-      V.ghost_blocks = blocks_with_absent_neighbour(S);
+      blocks_with_absent_neighbour(S, V.ghost_blocks, V.ghost_work);
       std::vector<int32_t> gi((size_t)S.n_blocks, -1);
       for (size_t r = 0; r < V.ghost_blocks.size(); ++r) gi[V.ghost_blocks[r]] = (int32_t)r;
       if ((rc = upload(&V.gidx, gi.data(), gi.size()))) return rc;
       const int sc = 1 << l;
-      V.edge_blocks = blocks_with_domain_edge(S, V.ghost_blocks, cd->nx * sc, cd->ny * sc,
-                                              cd->nz * sc);
+      blocks_with_domain_edge(S, cd->nx * sc, cd->ny * sc, cd->nz * sc, V.edge_blocks,
+                              V.edge_work);
       if (!V.ghost_blocks.empty()) {
         const size_t gb = V.ghost_blocks.size() * kHaloEntries * sizeof(float);
         OL_CUDA(cudaMalloc(&V.ghost, gb));

@@ -133,3 +133,33 @@ def test_ghost_staging_table_is_consistent(tables):
         cx, cy, cz = _c(k)
         # the slot is the source of a pull of an in-block cell
         assert 0 <= x + cx < 8 and 0 <= y + cy < 8 and 0 <= z + cz < 8
+
+
+def test_ghost_visit_order_weights_count_the_loader_table(tables):
+    """The ghost pass visits blocks by their number of absent-neighbour pulls
+    (solver.ghost_block_lists; native.cu orders the block pool's lists the
+    same way): the per-direction weights are the loader table's counts of
+    pulls from each neighbour, and a list is ordered largest first, ties by
+    block id."""
+    from openludwig_b200 import solver as S
+    _, w, _, _ = tables
+    counts = np.bincount((w[:HALO] >> 5) & 31, minlength=27)
+    assert counts.tolist() == S._PULLS_FROM_NEIGHBOUR.tolist()
+
+    class Lvl:  # four blocks in a row along x; the middle ones see more
+        n_blocks = 4
+        map_x, map_y, map_z = [1, 2, 3, 4], [1, 1, 1, 1], [1, 1, 1, 1]
+    nbr = np.zeros((27, 4), np.int32)
+    for b in range(4):
+        nbr[13, b] = b + 1
+        if b > 0:
+            nbr[12, b] = b       # -x neighbour present
+        if b < 3:
+            nbr[14, b] = b + 2   # +x neighbour present
+    Lvl.neighbor_table = nbr.reshape(-1)
+    ghost, edge = S.ghost_block_lists(Lvl, (64, 8, 8))
+    # every block misses 24 neighbours; the end blocks also miss the x face
+    assert ghost.tolist() == [0, 3, 1, 2]
+    # in a 64 x 8 x 8 domain the y / z neighbours are outside, and so is block
+    # 0's -x neighbour (block 3's absent +x neighbour is inside)
+    assert edge.tolist() == [0, 1, 2, 3]
