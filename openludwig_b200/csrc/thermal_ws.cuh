@@ -10,8 +10,10 @@
 // loaded one block earlier (a neighbour's g, the precomputed ghost value, or
 // pull_boundary_thermal) into the slots of the cells that pull them, pull,
 // release the stage to the next copies and run the passive-scalar BGK update.
-// The update is light, so the kernel is bound by the bulk copies and the
-// stores; the one-CTA-per-block kernel stages through registers instead.
+// The update is light (about 990 instructions per cell), too short to hide a
+// block's copies behind the previous block's update, so there are two stages:
+// block j+1 lands while block j is pulled and updated.  The one-CTA-per-block
+// kernel stages through registers instead.
 // A solid cell bounces its own unstreamed g back (adiabatic or isothermal
 // wall); the stage does not keep a cell's own values once the out-of-block
 // sources are written, so a solid cell reads them from global memory.
