@@ -149,10 +149,12 @@ OL_API int ol_stream_collide(const ol_level_view *lv, const ol_parent_view *pv,
 /* Which kernel ol_stream_collide (and the block pool's stream-collide
  * launches) run; no reference counterpart (the reference has one kernel
  * launch shape).  OL_SC_KERNEL_BLOCK: one CTA per 8^3 block, synchronous
- * staging.  OL_SC_KERNEL_WS: one persistent CTA per SM whose loader warps
- * stage the next block while its consumer warps collide the current one
- * (cumulant operator, levels whose absent-neighbour values are ghost rows or
- * level-1 domain boundaries; other launches keep the per-block kernel).
+ * staging.  OL_SC_KERNEL_WS: one persistent CTA per SM whose producer warp
+ * bulk-copies the next block while its consumer warps collide the current
+ * one (cumulant operator, levels whose absent-neighbour values are ghost rows
+ * or level-1 domain boundaries; other launches keep the per-block kernel).
+ * The same choice applies to ol_thermal (FP32 thermal populations, two
+ * blocks in flight per SM).
  * OL_SC_KERNEL_AUTO (default): OL_SC_KERNEL_WS for FP32 populations where
  * it applies and the level has at least two blocks per SM.  Both kernels
  * stage the same values and run the same cell-update code: rho and u agree
